@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Benchmark: pair-interactions/s of the velocity-Verlet step on one B200.
+
+Workload (default): the ion mixture of MD 6.2.0's int_ion_mix.f at
+N = 55,296 (Z = {6,8,26} with number fractions {0.2,0.7,0.1}, A = 2Z,
+n = 7.18e-5 fm^-3, kappa = 0.5, effective Gamma = 150), all FP64.  One step
+is one newton(do_measurements) of vel_verlet_2.f: drift, force call over all
+N(N-1)/2 = 1,528,811,160 pairs, kick; it measures every --meas-every steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs its own replica box on its own GPU
+(replicas only: the path has no exchange step), the timed region is bracketed
+by barriers and the time is the max over ranks.  Rank 0 prints one JSON line.
+
+--impl reference times the reference's CPU algorithm, i.e. the OpenMP C
+restatement in oracle/ (the Fortran cannot be compiled on these machines), on
+all host cores, each step one force call over a bounded block of target rows
+of the same full-size box.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+# The reference's mixture loops use schedule(runtime) (int_ion_mix.f:159,223);
+# the CPU arms state the schedule they ran with and default it to static.
+os.environ.setdefault("OMP_SCHEDULE", "static")
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+BASELINE_METRIC = "pair-interactions/s mixed vs FP64 at <=1e-5 energy drift; served p99 latency"
+UNIT = "pair-interactions/s"
+# Algorithmic FP64 flops per unique pair (counted from the reference source,
+# int_ion_pure.f:186-200 / :145-168, +2 for the mixture's Z weights).
+FLOPS_PER_PAIR = {("mix", False): 30, ("mix", True): 47, ("ocp", False): 28, ("ocp", True): 45,
+                  ("nucleon", False): 33, ("nucleon", True): 50}
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["mix", "ocp", "nucleon"], default="mix")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--meas-every", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--no-companion", action="store_true",
+                    help="skip the mixed-precision companion measurement")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(kind, seed):
+    from yukawamd_b200 import configs
+    if kind == "mix":
+        return configs.ion_mixture_cfg(seed)
+    if kind == "ocp":
+        return configs.pure_ion_ocp(seed)
+    return configs.nucleon_matter(seed)
+
+
+def workload_desc(w, kind):
+    n = w.n
+    if kind == "mix":
+        return ("ion-mixture N=%d Z={6,8,26} fractions {0.2,0.7,0.1} A=2Z n=7.18e-5/fm^3 "
+                "kappa=0.5 Gamma_eff=150 (int_ion_mix.f)" % n)
+    if kind == "ocp":
+        return "pure-ion OCP N=%d Z=8 A=16 kappa=1 Gamma=175 (int_ion_pure.f)" % n
+    return "nucleon N=%d x_p=0.4 n_B=0.05/fm^3 kT=1 HPP + p-p Coulomb lambda=10 (int_nn.f)" % n
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (torch.distributed for barriers and the max over ranks)
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        self.torch = None
+
+    def init(self):
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.torch = torch
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            t = self.torch.ones(1, device="cuda")
+            self.torch.distributed.all_reduce(t)
+            self.torch.cuda.synchronize()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
+        self.torch.distributed.all_reduce(t, op=self.torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if not self.pg:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
+        self.torch.distributed.all_reduce(t)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.torch.distributed.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        for line in self.lines:
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 8:
+                continue
+            if self.uuid and self.uuid not in f[0]:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                  "sw_power_cap"), f[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def device_uuid(dev):
+    try:
+        import torch
+        return str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+
+def time_engine(w, precision, steps, warmup, meas_every, dist, flush=True):
+    """W untimed steps, then K timed steps; returns (ms_total, perf, launches)."""
+    from yukawamd_b200 import abi
+    from yukawamd_b200.engine import Engine, kernel_launch_count
+    prec = abi.YK_PREC_MIXED if precision == "mixed" else abi.YK_PREC_FP64
+    e = Engine(w, precision=prec, device=dist.local)
+    e.accel(True)                                  # md.F:69, initial forces
+    if warmup:
+        e.run(warmup, meas_every, series=False)
+    e.perf_enable(True, L2_FLUSH_BYTES if flush else 0)
+    dist.barrier()
+    l0 = kernel_launch_count()
+    e.run(steps, meas_every, series=False)
+    launches = kernel_launch_count() - l0
+    dist.barrier()
+    perf = e.perf_read()
+    e.perf_enable(False, 0)
+    return e, perf, launches
+
+
+def e2e_engine(w, steps, warmup, meas_every, dist):
+    """Public-API loop with host buffers: every step copies x and v from
+    page-locked host memory to the device, runs newton, and copies x, v back
+    (the sync the Fortran shim makes while the driver keeps host-side tnorm /
+    cancel_vcom / strain)."""
+    from yukawamd_b200.engine import Engine, host_register, host_unregister
+    e = Engine(w, device=dist.local)
+    e.accel(True)
+    x = np.ascontiguousarray(w.x.copy())
+    v = np.ascontiguousarray(w.v.copy())
+    host_register(x)
+    host_register(v)
+    try:
+        for s in range(warmup):
+            e.set_state(x=x, v=v)
+            e.newton((s + 1) % meas_every == 0 if meas_every else False)
+            e.get_into(x=x, v=v)
+        dist.barrier()
+        t0 = time.perf_counter()
+        for s in range(steps):
+            e.set_state(x=x, v=v)
+            sc = e.newton((s + 1) % meas_every == 0 if meas_every else False)
+            e.get_into(x=x, v=v)
+            _ = sc.ev
+        t1 = time.perf_counter()
+        dist.barrier()
+    finally:
+        host_unregister(x)
+        host_unregister(v)
+        e.close()
+    return (t1 - t0) * 1e3, 2 * 24 * w.n, 2 * 24 * w.n + 112
+
+
+def read_traffic(kernel_tag):
+    """DRAM bytes per force launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "force_%s.md" % kernel_tag)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_sample(w, kind, target_s=12.0):
+    """Time the oracle's OpenMP force loop (reference structure) on all host
+    cores over a block of target rows of the full-size box."""
+    from oracle.oracle import Oracle
+    cores = os.cpu_count() or 1
+    orc = Oracle("double", threads=cores)
+    p = w.yk_params()
+    n = w.n
+    mid = n // 2
+
+    def run(nrows):
+        orc.set_row_range(mid, mid + nrows)
+        t0 = time.perf_counter()
+        orc.accel(p, w.x, w.zii, w.aii, False)
+        dt = time.perf_counter() - t0
+        pairs = sum(n - 1 - i for i in range(mid, min(mid + nrows, n - 1)))
+        return dt, pairs
+
+    dt, pairs = run(64)                                   # calibration
+    rate = pairs / max(dt, 1e-6)
+    nrows = int(min(n // 2 - 1, max(64, target_s * rate / (n - mid))))
+    dt, pairs = run(nrows)
+    orc.set_row_range()
+    return {"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "one force-only call of the oracle's OpenMP loop (int_ion_mix.f "
+                      "structure, OMP_SCHEDULE=%s) over target rows %d..%d of the full N=%d box: "
+                      "%d pairs in %.2f s" % (os.environ.get("OMP_SCHEDULE", "static"), mid,
+                                             mid + nrows, n, pairs, dt)}
+
+
+def run_ours(args, dist):
+    from yukawamd_b200 import _lib
+    from yukawamd_b200.engine import peak_probe
+    kind = args.workload
+    w = make_workload(kind, args.seed + dist.rank)
+    pairs_step = w.pairs_per_step
+    K, W, me = args.steps, args.warmup, args.meas_every
+
+    uuid = device_uuid(dist.local)
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    e, perf, launches = time_engine(w, args.precision, K, W, me, dist)
+    clk = clocks.stop()
+    ms_local = perf.run_ms
+    ms = dist.max(ms_local)
+    value = dist.world * pairs_step * K / (ms * 1e-3)
+
+    # dominant kernel: the force kernel, timed live with events on its stream
+    force_ms = perf.force_ms / max(perf.force_calls, 1)
+    meas_frac = (K // me) / K if me else 0.0
+    fpp = (1 - meas_frac) * FLOPS_PER_PAIR[(kind, False)] + meas_frac * FLOPS_PER_PAIR[(kind, True)]
+    prec_kind = 1 if args.precision == "mixed" else 0
+    peak = peak_probe(dist.local, prec_kind)
+    achieved = fpp * pairs_step / (force_ms * 1e-3) / 1e12
+    tag = "%s_%s" % (kind, args.precision)
+    roofline = {"bound": "fp64" if prec_kind == 0 else "fp32", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": read_traffic(tag),
+                "kernel": "k_force_rows (force kernel), avg %.3f ms/launch over %d launches"
+                          % (force_ms, perf.force_calls),
+                "peak_source": "measured live by yk_peak_probe (%s FMA chain, all SMs)"
+                               % ("FP64" if prec_kind == 0 else "FP32"),
+                "flops_per_pair": fpp, "force_share_of_step": perf.force_ms / perf.run_ms}
+
+    out = {"metric": BASELINE_METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+           "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+           "data": "synthetic: numpy PCG64 seed %d (+rank), uniform positions, Maxwell "
+                   "velocities with zero momentum" % args.seed,
+           "config": {"workload": workload_desc(w, kind), "n": w.n,
+                      "pairs_per_step": pairs_step, "precision": args.precision,
+                      "integrator": "vel_verlet_2", "meas_every": me,
+                      "l2": "flushed: 256 MiB device memset before every timed step "
+                            "(inside the timed region)",
+                      "parallelism": "replicas x%d (one box per GPU, no collective)" % dist.world},
+           "roofline": roofline, "gpu_launches": launches, "clocks": clk}
+    e.close()
+
+    if not args.no_companion:
+        other = "mixed" if args.precision == "fp64" else "fp64"
+        e2, perf2, _ = time_engine(w, other, K, W, me, dist)
+        ms2 = dist.max(perf2.run_ms)
+        v2 = dist.world * pairs_step * K / (ms2 * 1e-3)
+        # force accuracy of the mixed form against FP64 on the same positions
+        from yukawamd_b200 import abi
+        from yukawamd_b200.engine import Engine
+        with Engine(w, device=dist.local) as a64, \
+                Engine(w, device=dist.local, precision=abi.YK_PREC_MIXED) as a32:
+            s64 = a64.accel(True)
+            s32 = a32.accel(True)
+            n = w.n
+            ferr = float(np.linalg.norm(a32.a[:3 * n] - a64.a[:3 * n]) /
+                         np.linalg.norm(a64.a[:3 * n]))
+            ev_err = abs(s32.ev - s64.ev) / abs(s64.ev)
+            px_err = abs(s32.px - s64.px) / abs(s64.px)
+        out[other] = {"value": v2, "ms_per_step": ms2 / K,
+                      "ratio_mixed_over_fp64": (v2 / value) if other == "mixed" else (value / v2),
+                      "force_rms_rel_err_vs_fp64": ferr, "ev_rel_err": ev_err,
+                      "px_rel_err": px_err}
+        e2.close()
+
+    if not args.no_e2e:
+        t_e2e, bi, bo = e2e_engine(w, K, W, me, dist)
+        t_e2e = dist.max(t_e2e)
+        out["e2e"] = {"value": dist.world * pairs_step * K / (t_e2e * 1e-3), "unit": UNIT,
+                      "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                      "ms_per_step": t_e2e / K,
+                      "path": "Engine.set_state(x,v) -> Engine.newton -> Engine.get_into(x,v), "
+                              "page-locked host buffers, wall clock"}
+
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_sample(w, kind)
+    return out
+
+
+def run_reference(args):
+    """The reference's CPU algorithm (OpenMP C restatement) on all host cores."""
+    from oracle.oracle import Oracle
+    kind = args.workload
+    w = make_workload(kind, args.seed)
+    n = w.n
+    p = w.yk_params()
+    cores = os.cpu_count() or 1
+    orc = Oracle("double", threads=cores)
+    mid = n // 2
+
+    def pairs_of(r0, r1):
+        return sum(n - 1 - i for i in range(r0, min(r1, n - 1)))
+
+    # size each step to ~3 s of CPU work so the whole run stays within minutes
+    orc.set_row_range(mid, mid + 64)
+    t0 = time.perf_counter()
+    orc.accel(p, w.x, w.zii, w.aii, False)
+    rate = pairs_of(mid, mid + 64) / max(time.perf_counter() - t0, 1e-6)
+    nrows = int(min(n // 2 - 1, max(64, 3.0 * rate / (n - mid))))
+    orc.set_row_range(mid, mid + nrows)
+    for _ in range(args.warmup):
+        orc.accel(p, w.x, w.zii, w.aii, False)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        orc.accel(p, w.x, w.zii, w.aii, False)
+        times.append(time.perf_counter() - t0)
+    orc.set_row_range()
+    pairs = pairs_of(mid, mid + nrows)
+    total = sum(times)
+    value = pairs * args.steps / total
+    sample = ("each step: one force-only call of the oracle's OpenMP loop (reference "
+              "structure: omp for over j per target i, omp single fold) over target rows "
+              "%d..%d of the full N=%d box = %d pairs" % (mid, mid + nrows, n, pairs))
+    return {"metric": BASELINE_METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: numpy PCG64 seed %d" % args.seed, "impl": "reference",
+            "config": {"workload": workload_desc(w, kind), "n": n, "precision": "fp64",
+                       "parallelism": "OpenMP %d threads" % cores},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+    dist = Dist()
+    dist.init()
+    try:
+        out = run_ours(args, dist)
+        if dist.rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,212 @@
+/*
+ * yukawa_engine.h -- C-ABI of the B200 force-and-integrate engine.
+ *
+ * The engine replaces the hot path of the MD 6.2.0 Fortran code (Berry and
+ * Horowitz, Indiana University): the O(N^2) minimum-image pair sums of
+ * int_ion_pure.f / int_ion_mix.f / int_nn.f and the velocity-Verlet updates of
+ * vel_verlet_1/2/3.f.  The Fortran driver talks to those routines through two
+ * argument-less entry points that read and write module globals
+ * (md_globals.f:153-172):
+ *
+ *     subroutine accel(do_measurements)     int_control.f:52-81
+ *     subroutine newton(do_measurements)    vel_verlet_2.f:18-120
+ *
+ * This header is the plain C surface that a thin ISO_C_BINDING shim binds in
+ * their place.  Every entry point takes plain host pointers and sizes, returns
+ * an int status (YK_OK = 0) and never aborts; the shim maps a non-zero status
+ * to md_exit(1, yk_last_error(ctx)), which is how the Fortran code reports
+ * every fatal error (md_utils.f:158-183).
+ *
+ * Array layouts are the Fortran ones, so the shim passes c_loc() of the module
+ * arrays unchanged:
+ *     x, v, vold   real(8) (3, 0:n-1)  -> double[3*n]      x0,y0,z0,x1,...
+ *     a            real(8) (3, 0:n+2)  -> double[3*(n+3)]  columns n..n+2 hold
+ *                                         the packed raw sums that the
+ *                                         reference passes through its single
+ *                                         MPI_allreduce (int_ion_pure.f:217-226)
+ *     zii, aii     real(8) (0:n-1)     -> double[n]
+ *     pp           real(8) (3,3)       -> double[9] column-major
+ *
+ * All device state (positions, velocities, old velocities, accelerations,
+ * charges, masses) stays resident in HBM between calls.  Host arrays are read
+ * only by yk_create / yk_set_state and written only by yk_get_state and by the
+ * a_out argument of yk_accel.
+ */
+#ifndef YUKAWA_ENGINE_H
+#define YUKAWA_ENGINE_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define YK_API __attribute__((visibility("default")))
+#else
+#define YK_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define YK_OK               0
+#define YK_ERR_ARG          1   /* bad argument: n < 1, NULL pointer, dt <= 0 ... */
+#define YK_ERR_CUDA         2   /* a CUDA runtime call failed                    */
+#define YK_ERR_NOMEM        3   /* device allocation refused / admission refused */
+#define YK_ERR_STATE        4   /* call out of order (e.g. destroyed context)    */
+#define YK_ERR_TIMEOUT      5   /* a bounded device-side wait gave up            */
+#define YK_ERR_NONFINITE    6   /* NaN / Inf in an input array                   */
+#define YK_ERR_UNSUPPORTED  7   /* option not available in this build            */
+
+/* ---- simulation types: the cases of accel's select (int_control.f:69-87) */
+#define YK_SIM_NUCLEON      1   /* 'nucleon'      -> accel_nn        */
+#define YK_SIM_PURE_ION     2   /* 'pure-ion'     -> accel_ion_pure  */
+#define YK_SIM_ION_MIXTURE  3   /* 'ion-mixture'  -> accel_ion_mix   */
+#define YK_SIM_BFIELD       4   /* 'B-field'      -> a = 0           */
+
+/* ---- arithmetic of the pair terms -------------------------------------- */
+#define YK_PREC_FP64        0   /* all FP64: the drop-in form                    */
+#define YK_PREC_MIXED       1   /* FP64 positions, velocities, Verlet update and
+                                   minimum-image displacement; FP32 pair terms
+                                   with compensated (two-sum) accumulation      */
+
+/* ---- integrators -------------------------------------------------------- */
+#define YK_VV1              1   /* vel_verlet_1.f: two half kicks              */
+#define YK_VV2              2   /* vel_verlet_2.f: the linked one (default)    */
+#define YK_VV3              3   /* vel_verlet_3.f: Spreiter-Walter B-field     */
+
+/* ---- ion-mixture last-particle charge factor (int_ion_mix.f:158,201) ---- */
+#define YK_MIX_COMPAT       0   /* as the reference: a(:,n-1) lacks zii(n-1)   */
+#define YK_MIX_FIXED        1   /* physically correct: every a(:,i) has zii(i) */
+
+/*
+ * Run parameters: the md_globals module variables that accel / newton read
+ * (md_globals.f:36-140).  yk_params_default() fills the reference defaults.
+ */
+typedef struct yk_params {
+    int    sim_type;      /* YK_SIM_*                                         */
+    int    precision;     /* YK_PREC_*                                        */
+    int    integrator;    /* YK_VV1 / YK_VV2 / YK_VV3                         */
+    int    mix_mode;      /* YK_MIX_COMPAT / YK_MIX_FIXED                     */
+    int    coulomb_on;    /* coulomb == 'screened-coulomb'  (int_nn.f:167)   */
+    int    nuclear_on;    /* nuclear == 'HPP'               (int_nn.f:168)   */
+    int    device;        /* CUDA device ordinal                              */
+    int    reserved0;
+    double xl[3];         /* box edge lengths (fm)                            */
+    double rccut;         /* screened-Coulomb cutoff radius (fm), default 1e50 */
+    double rncut;         /* nuclear cutoff radius (fm)                       */
+    double xmuc;          /* inverse screening length 1/lambda (1/fm)         */
+    double vc;            /* Coulomb coupling alpha*hbar*c (MeV fm)           */
+    double frp;           /* ion form factor                                  */
+    double xmass;         /* nucleon mass (MeV)                               */
+    double rho;           /* particle density (1/fm^3)                        */
+    double kT;            /* temperature (MeV)                                */
+    double dt;            /* time step (fm/c)                                 */
+    double bfield;        /* uniform B field along z (Gauss)                  */
+    double zi, ai;        /* pure-ion charge and mass numbers                 */
+    double aa, bb, cc;    /* HPP nuclear parameters (MeV)                     */
+    double xpacket;       /* HPP Lambda (fm^2)                                */
+    double time;          /* simulation clock (fm/c)                          */
+} yk_params;
+
+/*
+ * Scalar outputs of accel / newton: the md_globals variables ev, vir, px, ek,
+ * pp(3,3) and time.  pp is column-major like the Fortran array.
+ */
+typedef struct yk_scalars {
+    double ev;            /* potential energy per particle (MeV)   */
+    double vir;           /* virial sum                             */
+    double px;            /* instantaneous pressure (MeV/fm^3)      */
+    double ek;            /* kinetic energy per particle (MeV)      */
+    double pp[9];         /* pressure tensor                        */
+    double time;          /* simulation clock after the call        */
+} yk_scalars;
+
+typedef struct yk_ctx yk_ctx;
+
+/* Fill *p with the reference defaults of md_globals.f:115-140
+ * (vc = ALPHA*HBARC, xmass = 931, rccut = 1e50, aa/bb/cc/xpacket = HPP, ...). */
+YK_API int yk_params_default(yk_params* p);
+
+/* Create an engine for n particles and copy the initial state to the device.
+ * Replaces the allocate/bcast block of input1.F:379-407 for the device side.
+ * v may be NULL (zero velocities).  zii / aii may be NULL for pure-ion runs
+ * (then every particle has zi / ai).  The arrays are copied, not retained. */
+YK_API int yk_create(const yk_params* p, int n,
+              const double* x, const double* v,
+              const double* zii, const double* aii,
+              yk_ctx** out);
+
+YK_API int yk_destroy(yk_ctx* ctx);
+
+/* Message of the last failed call on ctx (static string if ctx is NULL). */
+YK_API const char* yk_last_error(const yk_ctx* ctx);
+
+/* Force call: replaces accel(do_measurements), int_control.f:52-81.
+ * Computes accelerations from the device-resident positions.  If a_out is not
+ * NULL it receives a(3,0:n+2) exactly as the reference leaves it: scaled
+ * accelerations in columns 0..n-1 and the raw packed sums (ev, vir, 0, pxx,
+ * pxy, pxz, pyy, pyz, pzz) in columns n..n+2.  out may be NULL. */
+YK_API int yk_accel(yk_ctx* ctx, int do_meas, double* a_out, yk_scalars* out);
+
+/* One integrator step: replaces newton(do_measurements), vel_verlet_2.f:18
+ * (or vel_verlet_1.f:16 / vel_verlet_3.f:20 by params.integrator).  Works on
+ * the device-resident state; nothing is copied to or from host arrays. */
+YK_API int yk_newton(yk_ctx* ctx, int do_meas, yk_scalars* out);
+
+/* nsteps integrator steps back to back on the device, launched as CUDA graphs.
+ * Step s (1-based) measures when meas_every > 0 and s % meas_every == 0.
+ * series, if not NULL, receives nsteps yk_scalars (zeros on non-measuring
+ * steps, as the reference leaves them).  One host synchronisation at the end. */
+YK_API int yk_run(yk_ctx* ctx, int nsteps, int meas_every, yk_scalars* series);
+
+/* Host <-> device state sync points (before save_config / checkpoint /
+ * dump_data and around host-side tnorm / cancel_vcom / strain).  Any pointer
+ * may be NULL to skip that array.  a is double[3*n] (columns 0..n-1). */
+YK_API int yk_get_state(yk_ctx* ctx, double* x, double* v, double* vold, double* a);
+YK_API int yk_set_state(yk_ctx* ctx, const double* x, const double* v,
+                 const double* vold, const double* a);
+
+/* New box edge lengths (strain.f changes xl every step). */
+YK_API int yk_set_box(yk_ctx* ctx, const double xl[3]);
+
+/*
+ * Timers, the counterpart of the reference's perf.f report (perf.f:60-178:
+ * 'newton', 'accel' and 'calc_a' wall-clock timers).  With yk_perf_enable(ctx,
+ * 1, flush_bytes) the following yk_run calls launch step by step (no graph)
+ * with a CUDA event pair around every force kernel and around the whole run,
+ * and, if flush_bytes > 0, overwrite a device buffer of that size before every
+ * step so that no step starts from a warm L2.  yk_perf_read returns the sums
+ * since the last enable.
+ */
+typedef struct yk_perf {
+    double run_ms;            /* event time of the yk_run calls           */
+    double force_ms;          /* event time of the force kernels          */
+    long long steps;          /* integrator steps timed                   */
+    long long force_calls;    /* force kernels timed                      */
+} yk_perf;
+
+YK_API int yk_perf_enable(yk_ctx* ctx, int enable, size_t flush_bytes);
+YK_API int yk_perf_read(yk_ctx* ctx, yk_perf* out);
+
+/* Measured peak of a pipe on device `device`: kind 0 = FP64 FMA, kind 1 =
+ * FP32 FMA, in TFLOP/s (2 flops per FMA), from a register-resident FMA chain
+ * over the whole GPU.  Used for roofline denominators. */
+YK_API int yk_peak_probe(int device, int kind, double* tflops);
+
+/* Page-lock a caller-owned host buffer so that yk_get_state / yk_set_state
+ * copy it by DMA.  Optional. */
+YK_API int yk_host_register(void* ptr, size_t bytes);
+YK_API int yk_host_unregister(void* ptr);
+
+/* Number of kernels this library has launched in this process (all contexts).
+ * Used by benchmarks to report how much device work a measured region did. */
+YK_API unsigned long long yk_kernel_launch_count(void);
+
+/* Library version string. */
+YK_API const char* yk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YUKAWA_ENGINE_H */

@@ -1,0 +1,237 @@
+"""GPU parity: the CUDA engine through the C-ABI against the CPU oracle.
+
+Tolerances (stated here, used below):
+  FP64 form   forces  ||a_gpu - a_ref||_2 / ||a_ref||_2 <= 1e-12
+              ev, vir, px relative <= 1e-12; pp and the packed raw sums
+              a(:,n..n+2) by 2-norm <= 1e-12
+              Verlet positions / velocities: bit-identical given identical
+              accelerations ('B-field' force case)
+  mixed form  forces 2-norm relative <= 1e-6; ev, px relative <= 1e-6;
+              pp 2-norm relative <= 1e-5
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from yukawamd_b200 import abi, configs
+from yukawamd_b200.engine import Engine, kernel_launch_count
+
+from helpers import params_from_dict, rel, rel_norm
+from rows import row_accels
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIX_F_TOL = 1e-6
+MIX_S_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return Oracle("double", threads=8)
+
+
+def workload(kind, n, seed):
+    if kind == "pure":
+        return configs.pure_ion_ocp(seed, n)
+    if kind == "mix":
+        return configs.ion_mixture_cfg(seed, n)
+    return configs.nucleon_matter(seed, n)
+
+
+def check_accel(orc, w, prec, meas, mix_mode=abi.YK_MIX_COMPAT, gpu=None):
+    p = w.yk_params(precision=prec, mix_mode=mix_mode)
+    n = w.n
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        s = e.accel(meas)
+        a_gpu = e.a.copy()
+    a_ref, s_ref = orc.accel(p, w.x, w.zii, w.aii, meas)
+    if prec == abi.YK_PREC_FP64:
+        ft, st, pt = FP64_TOL, FP64_TOL, FP64_TOL
+    else:
+        ft, st, pt = MIX_F_TOL, MIX_S_TOL, 1e-5
+    assert rel_norm(a_gpu[:3 * n], a_ref[:3 * n]) <= ft
+    if meas:
+        assert rel_norm(a_gpu[3 * n:], a_ref[3 * n:]) <= pt
+        assert rel(s.ev, s_ref.ev) <= st
+        assert rel(s.vir, s_ref.vir) <= st
+        assert rel(s.px, s_ref.px) <= st
+        assert rel_norm(np.array(s.pp), np.array(s_ref.pp)) <= pt
+    else:
+        assert np.all(a_gpu[3 * n:] == 0.0)
+        assert s.ev == 0.0 and s.px == 0.0 and all(t == 0.0 for t in s.pp)
+
+
+@pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("meas", [True, False], ids=["meas", "force"])
+@pytest.mark.parametrize("kind,n", [("pure", 4096), ("mix", 3000), ("nn", 3000)])
+def test_accel_matches_oracle(gpu, orc, kind, n, meas, prec):
+    check_accel(orc, workload(kind, n, 100 + n), prec, meas)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 127, 128, 129, 255, 257])
+@pytest.mark.parametrize("kind", ["pure", "mix", "nn"])
+def test_ragged_sizes(gpu, orc, kind, n):
+    w = workload(kind, n, 7 + n)
+    check_accel(orc, w, abi.YK_PREC_FP64, True)
+    check_accel(orc, w, abi.YK_PREC_FP64, False)
+
+
+@pytest.mark.parametrize("mode", [abi.YK_MIX_COMPAT, abi.YK_MIX_FIXED], ids=["compat", "fixed"])
+def test_mix_last_particle_mode(gpu, orc, mode):
+    check_accel(orc, workload("mix", 513, 5), abi.YK_PREC_FP64, False, mix_mode=mode)
+
+
+def test_known_answers_through_capi(gpu):
+    import json
+    import os
+    doc = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "kat.json")))
+    for case in doc["accel"]:
+        p = params_from_dict(case["params"])
+        n = len(case["zii"])
+        with Engine(p, np.array(case["x"]), None, np.array(case["zii"]),
+                    np.array(case["aii"])) as e:
+            s = e.accel(case["do_meas"])
+            a = e.a.copy()
+        ref = np.array(case["a"])
+        assert rel_norm(a[:3 * n], ref[:3 * n]) <= 1e-14, case["name"]
+        if case["do_meas"]:
+            assert rel_norm(a[3 * n:], ref[3 * n:]) <= 1e-14, case["name"]
+            assert rel(s.ev, case["ev"]) <= 1e-14
+            assert rel(s.px, case["px"]) <= 1e-14
+
+
+@pytest.mark.parametrize("integ", [1, 2, 3])
+@pytest.mark.parametrize("bfield", [0.0, 2.0e17], ids=["b0", "b1"])
+def test_verlet_bit_exact(gpu, orc, integ, bfield):
+    """'B-field' force case (a = 0): every step's x, v, vold, a must be
+    bit-identical to the oracle's reference-order arithmetic."""
+    w = configs.ion_mixture_cfg(31, 1000)
+    p = w.yk_params(sim_type=abi.YK_SIM_BFIELD, integrator=integ, bfield=bfield)
+    n = w.n
+    rng = np.random.default_rng(3)
+    a0 = rng.standard_normal(3 * n) * 1e-4
+    x, v = w.x.copy(), w.v.copy()
+    vold = np.zeros(3 * n)
+    a = np.zeros(3 * (n + 3))
+    a[:3 * n] = a0
+    s_ref = abi.YkScalars()
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        e.set_state(a=a0)
+        for step in range(4):
+            meas = step % 2 == 1
+            s = e.newton(meas)
+            orc.newton(p, x, v, vold, a, w.zii, w.aii, meas, s_ref)
+            gx, gv, gvold, ga = e.get_state()
+            assert np.array_equal(gx, x)
+            assert np.array_equal(gv, v)
+            assert np.array_equal(ga, a[:3 * n])
+            if integ == 2:
+                assert np.array_equal(gvold, vold)
+            assert rel(s.ek, s_ref.ek) <= 1e-13
+            assert rel_norm(np.array(s.pp), np.array(s_ref.pp)) <= 1e-13
+            assert s.time == s_ref.time
+
+
+@pytest.mark.parametrize("kind", ["pure", "mix", "nn"])
+def test_newton_steps_match_oracle(gpu, orc, kind):
+    w = workload(kind, 1500, 41)
+    p = w.yk_params()
+    n = w.n
+    x, v = w.x.copy(), w.v.copy()
+    vold = np.zeros(3 * n)
+    a, s_ref = orc.accel(p, x, w.zii, w.aii, True)
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        e.accel(True)
+        for step in range(5):
+            meas = step >= 3
+            s = e.newton(meas)
+            orc.newton(p, x, v, vold, a, w.zii, w.aii, meas, s_ref)
+        gx, gv, _, ga = e.get_state()
+    assert rel_norm(gx, x) <= 1e-14
+    assert rel_norm(gv, v) <= 1e-12
+    assert rel_norm(ga, a[:3 * n]) <= 1e-11
+    assert rel(s.ev, s_ref.ev) <= 1e-11
+    assert rel(s.ek, s_ref.ek) <= 1e-11
+    assert rel(s.px, s_ref.px) <= 1e-11
+
+
+@pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
+def test_run_graph_equals_newton_loop(gpu, prec):
+    """yk_run (CUDA graphs) is bit-identical to the same steps via yk_newton."""
+    w = configs.pure_ion_ocp(51, 2000)
+    p = w.yk_params(precision=prec)
+    steps, me = 57, 5
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e1:
+        e1.accel(True)
+        ser1 = [abi.YkScalars.from_buffer_copy(e1.newton((k + 1) % me == 0)) for k in range(steps)]
+        st1 = e1.get_state()
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e2:
+        e2.accel(True)
+        ser2 = e2.run(steps, me)
+        st2 = e2.get_state()
+    for A, B in zip(st1, st2):
+        assert np.array_equal(A, B)
+    for s1, s2 in zip(ser1, ser2):
+        assert bytes(s1) == bytes(s2)
+
+
+def test_full_size_rows_and_third_law(gpu):
+    """N = 55,296 ion mixture (the benchmark size): sampled rows against a
+    numpy restatement, Newton's third law on the FP64 forces, and the mixed
+    form against FP64."""
+    w = configs.ion_mixture_cfg(2)
+    n = w.n
+    p = w.yk_params(mix_mode=abi.YK_MIX_FIXED)
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        e.accel(True)
+        a64 = e.a[:3 * n].copy()
+    rows = np.random.default_rng(1).choice(n, 48, replace=False)
+    ref = row_accels(p, w.x, w.zii, w.aii, rows)
+    got = a64.reshape(-1, 3)[rows]
+    assert rel_norm(got, ref) <= FP64_TOL
+    F = a64.reshape(-1, 3) * (w.aii[:, None] * p.xmass)
+    assert np.all(np.abs(F.sum(0)) <= 1e-11 * np.abs(F).sum(0))
+    with Engine(p, w.x, w.v, w.zii, w.aii, precision=abi.YK_PREC_MIXED) as e:
+        e.accel(True)
+        am = e.a[:3 * n].copy()
+    assert rel_norm(am, a64) <= MIX_F_TOL
+
+
+def test_state_round_trip_and_box(gpu, orc):
+    w = configs.pure_ion_ocp(61, 700)
+    p = w.yk_params()
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        x, v, vold, a = e.get_state()
+        assert np.array_equal(x, w.x) and np.array_equal(v, w.v)
+        L2 = [t * 1.01 for t in p.xl]
+        e.set_box(L2)
+        x2 = w.x * 1.01
+        e.set_state(x=x2)
+        s = e.accel(True)
+        p2 = w.yk_params()
+        for k in range(3):
+            p2.xl[k] = L2[k]
+        a_ref, s_ref = orc.accel(p2, x2, w.zii, w.aii, True)
+        assert rel_norm(e.a[:3 * w.n], a_ref[:3 * w.n]) <= FP64_TOL
+        assert rel(s.ev, s_ref.ev) <= FP64_TOL
+
+
+def test_kernels_actually_launch(gpu):
+    w = configs.pure_ion_ocp(71, 300)
+    before = kernel_launch_count()
+    with Engine(w) as e:
+        e.accel(True)
+        e.newton(False)
+        e.run(10, 0, series=False)
+    assert kernel_launch_count() - before >= 2 + 4 + 40
+
+
+def test_nonfinite_state_rejected(gpu):
+    w = configs.pure_ion_ocp(72, 100)
+    with Engine(w) as e:
+        bad = w.x.copy()
+        bad[5] = np.nan
+        with pytest.raises(Exception) as ei:
+            e.set_state(x=bad)
+        assert ei.value.code == abi.YK_ERR_NONFINITE

@@ -1,0 +1,200 @@
+// yk_common.cuh -- device helpers shared by the engine's kernels (sm_100a).
+//
+//  * 1-D TMA bulk copies global -> shared (cp.async.bulk) completed on an
+//    mbarrier, with bounded waits that report a timeout instead of hanging.
+//    No multicast form is used anywhere in this engine.
+//  * warp / block reductions of double partial sums in a fixed order, so
+//    every result is bit-reproducible run to run.
+//  * compensated FP32 accumulation (Knuth two-sum) for the mixed form.
+//  * an FP32 exp(-t) built from Cody-Waite reduction and a polynomial for
+//    2^f on [-1/2, 1/2] (relative-error least-squares fit with Lawson
+//    reweighting on 4001 Chebyshev nodes; tests/test_numerics.py re-runs the
+//    fit and checks the error bound).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace yk {
+
+// Bits of the device error word.
+constexpr unsigned ERR_TIMEOUT = 1u << 0;   // a bounded mbarrier wait gave up
+constexpr unsigned ERR_BOUNDS  = 1u << 1;   // an index check failed (debug builds)
+
+// Iteration bound of every spin on an mbarrier.  One try_wait suspends the
+// thread for a hardware time slice; a j-tile lands in a few microseconds, so
+// the bound is only ever reached if a copy never completes.
+constexpr long long SPIN_LIMIT = 1ll << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// 1-D bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned)
+// from this GPU's global memory into this CTA's shared memory.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of *bar with at most SPIN_LIMIT polls.  Returns
+// false (and sets ERR_TIMEOUT in *err) if the phase never completed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* err)
+{
+    for (long long it = 0; it < SPIN_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(err, ERR_TIMEOUT);
+    return false;
+}
+
+// ---- reductions ----------------------------------------------------------
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum K values over the block in a fixed order; the result lands in out[k]
+// (global) from thread 0.  scratch: shared double[32*K].
+template <int K>
+__device__ __forceinline__ void block_sum_store(double (&v)[K], double* scratch, double* out)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = warp_sum(v[k]);
+        if (lane == 0) scratch[warp * K + k] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < nwarps ? scratch[lane * K + k] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) out[k] = s;
+        }
+    }
+}
+
+// ---- compensated FP32 sums ---------------------------------------------
+
+// Knuth two-sum: s + c carries the running sum; the rounding error of every
+// addition is captured exactly in c (6 flops, no branch).
+struct cf32 {
+    float s, c;
+    __device__ __forceinline__ cf32() : s(0.f), c(0.f) {}
+    __device__ __forceinline__ void add(float x)
+    {
+        float t = __fadd_rn(s, x);
+        float bp = __fsub_rn(t, s);
+        float e = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(x, bp));
+        s = t;
+        c = __fadd_rn(c, e);
+    }
+    __device__ __forceinline__ double value() const { return (double)s + (double)c; }
+};
+
+// Kahan sum for sums of one sign (energies, virial): 4 flops.
+struct kf32 {
+    float s, c;
+    __device__ __forceinline__ kf32() : s(0.f), c(0.f) {}
+    __device__ __forceinline__ void add(float x)
+    {
+        float y = __fsub_rn(x, c);
+        float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// ---- FP32 exp(-t), t >= 0 ---------------------------------------------
+// e^{-t} = 2^{y}, y = -t log2(e) = k + f, |f| <= 1/2.  y is formed with the
+// product's rounding error recovered by an FMA (Cody-Waite style), so f is
+// accurate to ~1e-9 absolute; 2^f comes from a degree-6 polynomial fitted
+// on [-1/2, 1/2] (2e-9 relative in exact arithmetic, 1e-7 = 1.7 ulp with
+// FP32 Horner rounding); 2^k is applied through
+// the exponent bits.  Results below 2^-126 flush to zero.
+__device__ __forceinline__ float exp_neg_f32(float t)
+{
+    const float L2E_HI = 1.44269502162933349609375f;      // float(log2 e)
+    const float L2E_LO = 1.925963033500011079e-8f;       // log2 e - L2E_HI
+    float yh = -t * L2E_HI;
+    float yl = fmaf(-t, L2E_HI, -yh);                    // exact error of -t*L2E_HI
+    yl = fmaf(-t, L2E_LO, yl);
+    float k = rintf(yh);
+    float f = (yh - k) + yl;                             // yh - k is exact
+    // 2^f = sum c_m f^m, c_m fitted to 2^f on [-0.5, 0.5]
+    float p = 1.5353360504377633e-4f;
+    p = fmaf(p, f, 1.3398875016719103e-3f);
+    p = fmaf(p, f, 9.6184369176626205e-3f);
+    p = fmaf(p, f, 5.5503323674201965e-2f);
+    p = fmaf(p, f, 2.4022647738456726e-1f);
+    p = fmaf(p, f, 6.9314718246459961e-1f);
+    p = fmaf(p, f, 1.0f);
+    int ki = (int)k;
+    float r = __int_as_float(__float_as_int(p) + (ki << 23));
+    return (k < -125.f) ? 0.f : r;
+}
+
+// FP32 1/sqrt(x): hardware estimate plus one Newton step.
+__device__ __forceinline__ float rsqrt_f32(float x)
+{
+    float y = rsqrtf(x);
+    float h = __fmul_rn(0.5f * x, y);
+    return __fmul_rn(y, fmaf(-h, y, 1.5f));
+}
+
+// Minimum image of a displacement d in [-L, L] exactly as the reference's
+// pair of conditional corrections (int_ion_pure.f:149-150): d - L if d > L/2,
+// d + L if d < -L/2.  The comparisons run on the bit patterns (valid because
+// L/2 > 0 and d is finite), which keeps them off the FP64 pipe.
+__device__ __forceinline__ double min_image(double d, double L, long long hl_bits)
+{
+    const long long b = __double_as_longlong(d);
+    double s = 0.0;
+    if (b > hl_bits) s = -L;
+    else if ((b ^ (long long)0x8000000000000000ull) > hl_bits) s = L;
+    return __dadd_rn(d, s);
+}
+
+}  // namespace yk

@@ -1,0 +1,818 @@
+// yk_engine.cu -- the C-ABI of include/yukawa_engine.h.
+//
+// One yk_ctx per simulation box.  Device state stays resident between calls:
+// x, v, vold, a (Fortran layout), zii, aii, the packed double4 positions the
+// force kernels stream, per-CTA partial sums and the md_globals scalars.
+// Every call runs on the context's own stream; calls that return results to
+// the host synchronise that stream once at the end.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/yukawa_engine.h"
+#include "yk_force.cuh"
+#include "yk_verlet.cuh"
+
+using namespace yk;
+
+static std::atomic<unsigned long long> g_launches{0};
+
+// FMA-throughput probe: PROBE_CHAINS independent dependent chains per thread.
+constexpr int PROBE_CHAINS = 8;
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b)
+{
+    T x[PROBE_CHAINS];
+#pragma unroll
+    for (int q = 0; q < PROBE_CHAINS; ++q) x[q] = (T)(threadIdx.x + q);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int q = 0; q < PROBE_CHAINS; ++q) x[q] = fma(x[q], a, b);
+    }
+    T s = 0;
+#pragma unroll
+    for (int q = 0; q < PROBE_CHAINS; ++q) s += x[q];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+static thread_local std::string g_err_noctx;
+
+#define YK_VERSION_STR "yukawamd_b200 0.1.0 (sm_100a)"
+
+struct yk_ctx {
+    yk_params p;
+    int n = 0;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    double *x = nullptr, *v = nullptr, *vold = nullptr, *a = nullptr;
+    double *zii = nullptr, *aii = nullptr;
+    double4* pos = nullptr;
+    double *fpart = nullptr, *kpart = nullptr;
+    DevScalars* ds = nullptr;
+    unsigned* err = nullptr;
+    double* series = nullptr;
+    int series_cap = 0;
+    int* series_idx = nullptr;
+    DevScalars* h_ds = nullptr;     // pinned staging for scalars + error word
+    unsigned* h_err = nullptr;
+    ForceArgs fa{};
+    StepArgs sa{};
+    FinishArgs fz_base{};
+    int nfb = 0, nvb = 0;
+    double time = 0.0;
+    bool pos_dirty = true;
+    // perf timers (yk_perf_enable)
+    bool perf_on = false;
+    size_t flush_bytes = 0;
+    unsigned char* flush_buf = nullptr;
+    std::vector<cudaEvent_t> ev_pool;
+    int ev_used = 0;
+    yk_perf perf{};
+    // cached K-step graph
+    cudaGraphExec_t graph = nullptr;
+    int graph_K = 0, graph_me = -1, graph_series = -1, graph_kernels = 0;
+    std::string errmsg;
+};
+
+static int fail(yk_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c)
+        c->errmsg = buf;
+    else
+        g_err_noctx = buf;
+    return code;
+}
+
+#define CK(ctx, call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail((ctx), YK_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// parameters -> kernel argument blocks
+
+static double ev_cut(const yk_params& p, double scale)
+{
+    // int_ion_pure.f:125-130 (scale 1), int_nn.f:177-182 (scale vc)
+    const double* xl = p.xl;
+    if (p.rccut <= std::sqrt(xl[0] * xl[0] + xl[1] * xl[1] + xl[2] * xl[2]) / 2.0)
+        return scale * std::exp(-(p.xmuc * p.rccut)) / p.rccut;
+    return 0.0;
+}
+
+static void setup_args(yk_ctx* c)
+{
+    const yk_params& p = c->p;
+    ForceArgs& f = c->fa;
+    f = ForceArgs{};
+    for (int k = 0; k < 3; ++k) {
+        f.xl[k] = p.xl[k];
+        const double hl = 0.5 * p.xl[k];
+        std::memcpy(&f.hlb[k], &hl, sizeof hl);
+    }
+    f.rc2 = p.rccut * p.rccut;
+    f.rn2 = p.rncut * p.rncut;
+    f.xmuc = p.xmuc;
+    f.vc = p.vc;
+    f.evcut = (p.sim_type == YK_SIM_NUCLEON) ? ev_cut(p, p.vc) : ev_cut(p, 1.0);
+    f.xpi = 1. / p.xpacket;
+    f.xp2i = 1. / (2. * p.xpacket);
+    f.aa = p.aa;
+    f.aa2 = 2. * p.aa;
+    f.bpc = p.bb + p.cc;
+    f.bmc = p.bb - p.cc;
+    if (p.sim_type == YK_SIM_PURE_ION)
+        f.coef = p.frp * p.zi * p.zi * p.vc;
+    else if (p.sim_type == YK_SIM_ION_MIXTURE)
+        f.coef = p.frp * p.vc;
+    else
+        f.coef = 1.0;
+    f.xmass = p.xmass;
+    f.ai_xmass = p.ai * p.xmass;
+    f.rc2f = (float)f.rc2;
+    f.rn2f = (float)f.rn2;
+    f.xmucf = (float)f.xmuc;
+    f.evcutf = (float)f.evcut;
+    f.vcf = (float)f.vc;
+    f.xpif = (float)f.xpi;
+    f.xp2if = (float)f.xp2i;
+    f.aaf = (float)f.aa;
+    f.aa2f = (float)f.aa2;
+    f.bpcf = (float)f.bpc;
+    f.bmcf = (float)f.bmc;
+    f.n = c->n;
+    f.nuclear_on = p.nuclear_on;
+    f.coulomb_on = p.coulomb_on;
+    f.mix_compat = (p.mix_mode == YK_MIX_COMPAT);
+
+    StepArgs& s = c->sa;
+    s = StepArgs{};
+    for (int k = 0; k < 3; ++k) s.xl[k] = p.xl[k];
+    s.dt = p.dt;
+    s.afac = (p.integrator == YK_VV1) ? (0.5 * p.dt) * p.dt : 0.5 * (p.dt * p.dt);
+    s.halfdt = 0.5 * p.dt;
+    s.bfield = p.bfield;
+    s.lorentz_c = (p.integrator == YK_VV3) ? (double)3.218404e-20f : 3.218404e-20;
+    s.n = c->n;
+    s.pack_w = (p.sim_type == YK_SIM_ION_MIXTURE || p.sim_type == YK_SIM_NUCLEON) ? 1 : 0;
+
+    FinishArgs& z = c->fz_base;
+    z = FinishArgs{};
+    z.n = c->n;
+    z.half = 0.5;
+    z.coef = f.coef;
+    z.rho = p.rho;
+    z.kT = p.kT;
+    z.xmass = p.xmass;
+    z.vol = p.xl[0] * p.xl[1] * p.xl[2];
+    z.f_n = (double)(float)c->n;
+    z.f_3n = (double)(3.0f * (float)c->n);
+
+    c->nfb = (c->n + FBLOCK - 1) / FBLOCK;
+    c->nvb = (c->n + VBLOCK - 1) / VBLOCK;
+}
+
+static void drop_graph(yk_ctx* c)
+{
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_K = 0;
+    c->graph_me = -1;
+    c->graph_series = -1;
+    c->graph_kernels = 0;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers (all on c->stream; they only enqueue)
+
+template <int SIM, int PREC, bool MEAS>
+static void launch_force_t(yk_ctx* c)
+{
+    k_force_rows<SIM, PREC, MEAS><<<c->nfb, FBLOCK, FORCE_SMEM, c->stream>>>(
+        c->pos, c->aii, c->fa, c->a, c->fpart, c->err);
+}
+
+template <int SIM>
+static void launch_force_s(yk_ctx* c, bool meas)
+{
+    const bool mixed = c->p.precision == YK_PREC_MIXED;
+    if (mixed) {
+        if (meas) launch_force_t<SIM, PREC_MIXED, true>(c);
+        else launch_force_t<SIM, PREC_MIXED, false>(c);
+    } else {
+        if (meas) launch_force_t<SIM, PREC_FP64, true>(c);
+        else launch_force_t<SIM, PREC_FP64, false>(c);
+    }
+}
+
+static cudaEvent_t next_event(yk_ctx* c)
+{
+    if (c->ev_used == (int)c->ev_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+
+static int enqueue_force_body(yk_ctx* c, bool meas);
+
+// Returns the number of kernels enqueued.  Under yk_perf_enable the force
+// kernel is bracketed by an event pair (events are consumed in pairs).
+static int enqueue_force(yk_ctx* c, bool meas, bool timed = false)
+{
+    if (!timed) return enqueue_force_body(c, meas);
+    cudaEventRecord(next_event(c), c->stream);
+    int k = enqueue_force_body(c, meas);
+    cudaEventRecord(next_event(c), c->stream);
+    return k;
+}
+
+static int enqueue_force_body(yk_ctx* c, bool meas)
+{
+    switch (c->p.sim_type) {
+    case YK_SIM_PURE_ION: launch_force_s<SIM_PURE>(c, meas); return 1;
+    case YK_SIM_ION_MIXTURE: launch_force_s<SIM_MIX>(c, meas); return 1;
+    case YK_SIM_NUCLEON: launch_force_s<SIM_NUCLEON>(c, meas); return 1;
+    default:  // 'B-field': a = 0 (int_control.f:80-81)
+        cudaMemsetAsync(c->a, 0, sizeof(double) * 3 * (size_t)(c->n + 3), c->stream);
+        return 0;
+    }
+}
+
+static int enqueue_finish(yk_ctx* c, bool meas, int kin_mode, bool series)
+{
+    FinishArgs z = c->fz_base;
+    const bool has_force = c->p.sim_type != YK_SIM_BFIELD;
+    z.force_mode = has_force ? 1 : 0;
+    z.nfp = (has_force && meas) ? c->nfb : 0;
+    z.do_meas = meas ? 1 : 0;
+    z.kin_mode = kin_mode;
+    z.nkp = (kin_mode == 2) ? c->nvb : 0;
+    k_finish<<<1, 256, 0, c->stream>>>(c->fpart, c->kpart, z, c->a, c->ds,
+                                       series ? c->series : nullptr, c->series_idx);
+    return 1;
+}
+
+// One integrator step; returns kernels enqueued.
+static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool timed = false)
+{
+    int k = 0;
+    const int nb = c->nvb;
+    cudaStream_t st = c->stream;
+    const StepArgs& s = c->sa;
+    switch (c->p.integrator) {
+    case YK_VV1: k_drift_vv1<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->pos, s); break;
+    case YK_VV3: k_drift_vv3<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->aii, c->pos, s); break;
+    default: k_drift_vv2<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->vold, c->a, c->zii, c->pos, s); break;
+    }
+    ++k;
+    k += enqueue_force(c, meas, timed);
+    int kin_mode;
+    switch (c->p.integrator) {
+    case YK_VV1:
+        k_post_vv1<<<nb, VBLOCK, 0, st>>>(c->v, c->a, c->aii, c->kpart, s);
+        kin_mode = 2;
+        break;
+    case YK_VV3:
+        k_post_vv3<<<nb, VBLOCK, 0, st>>>(c->v, c->a, c->zii, c->aii, c->kpart, s);
+        kin_mode = 2;
+        break;
+    default: {
+        const bool bf = c->p.bfield != 0.0;
+        if (meas) {
+            if (bf) k_post_vv2<true, true><<<nb, VBLOCK, 0, st>>>(c->v, c->vold, c->a, c->zii, c->aii, c->kpart, s);
+            else k_post_vv2<true, false><<<nb, VBLOCK, 0, st>>>(c->v, c->vold, c->a, c->zii, c->aii, c->kpart, s);
+        } else {
+            if (bf) k_post_vv2<false, true><<<nb, VBLOCK, 0, st>>>(c->v, c->vold, c->a, c->zii, c->aii, c->kpart, s);
+            else k_post_vv2<false, false><<<nb, VBLOCK, 0, st>>>(c->v, c->vold, c->a, c->zii, c->aii, c->kpart, s);
+        }
+        kin_mode = meas ? 2 : 1;
+    }
+    }
+    ++k;
+    k += enqueue_finish(c, meas, kin_mode, series);
+    return k;
+}
+
+static int enqueue_pack(yk_ctx* c)
+{
+    if (!c->pos_dirty) return 0;
+    k_pack<<<c->nvb, VBLOCK, 0, c->stream>>>(c->x, c->zii, c->pos, c->n, c->sa.pack_w);
+    c->pos_dirty = false;
+    return 1;
+}
+
+// Copy scalars and the error word back and wait for the stream.
+static int sync_and_check(yk_ctx* c)
+{
+    CK(c, cudaMemcpyAsync(c->h_ds, c->ds, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaMemcpyAsync(c->h_err, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    CK(c, cudaGetLastError());
+    if (*c->h_err) {
+        unsigned e = *c->h_err;
+        cudaMemsetAsync(c->err, 0, sizeof(unsigned), c->stream);
+        cudaStreamSynchronize(c->stream);
+        if (e & ERR_TIMEOUT)
+            return fail(c, YK_ERR_TIMEOUT, "a device-side wait timed out (error word 0x%x)", e);
+        return fail(c, YK_ERR_CUDA, "device error word 0x%x", e);
+    }
+    return YK_OK;
+}
+
+static void fill_scalars(const yk_ctx* c, yk_scalars* out)
+{
+    if (!out) return;
+    const DevScalars& s = *c->h_ds;
+    out->ev = s.ev;
+    out->vir = s.vir;
+    out->px = s.px;
+    out->ek = s.ek;
+    for (int k = 0; k < 9; ++k) out->pp[k] = s.pp[k];
+    out->time = c->time;
+}
+
+static bool all_finite(const double* p, size_t cnt)
+{
+    for (size_t i = 0; i < cnt; ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+static int check_params(const yk_params* p)
+{
+    if (p->sim_type < YK_SIM_NUCLEON || p->sim_type > YK_SIM_BFIELD)
+        return fail(nullptr, YK_ERR_ARG, "sim_type %d is not one of 1..4", p->sim_type);
+    if (p->precision != YK_PREC_FP64 && p->precision != YK_PREC_MIXED)
+        return fail(nullptr, YK_ERR_ARG, "precision %d is not 0 or 1", p->precision);
+    if (p->integrator < YK_VV1 || p->integrator > YK_VV3)
+        return fail(nullptr, YK_ERR_ARG, "integrator %d is not 1..3", p->integrator);
+    if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, YK_ERR_ARG, "dt must be > 0");
+    for (int k = 0; k < 3; ++k)
+        if (!(p->xl[k] > 0.0) || !std::isfinite(p->xl[k]))
+            return fail(nullptr, YK_ERR_ARG, "box edge xl(%d) must be > 0", k + 1);
+    if (p->sim_type == YK_SIM_PURE_ION && !(p->ai > 0.0))
+        return fail(nullptr, YK_ERR_ARG, "pure-ion runs need ai > 0");
+    if (!(p->xmass > 0.0)) return fail(nullptr, YK_ERR_ARG, "xmass must be > 0");
+    if (p->sim_type == YK_SIM_NUCLEON && p->nuclear_on && !(p->xpacket > 0.0))
+        return fail(nullptr, YK_ERR_ARG, "xpacket must be > 0");
+    return YK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+
+extern "C" {
+
+const char* yk_version(void) { return YK_VERSION_STR; }
+
+unsigned long long yk_kernel_launch_count(void) { return g_launches.load(); }
+
+int yk_params_default(yk_params* p)
+{
+    if (!p) return YK_ERR_ARG;
+    std::memset(p, 0, sizeof *p);
+    p->sim_type = YK_SIM_PURE_ION;
+    p->precision = YK_PREC_FP64;
+    p->integrator = YK_VV2;
+    p->mix_mode = YK_MIX_COMPAT;
+    p->coulomb_on = 1;
+    p->nuclear_on = 0;
+    p->rccut = 1.0e50;                  // md_globals.f:120
+    p->vc = (1.0 / 137.036) * 197.327;  // ALPHA*HBARC, md_globals.f:122
+    p->frp = 1.0;
+    p->xmass = 931.00;
+    p->xpacket = 1.25;                  // md_globals.f:127-130
+    p->aa = 110.0;
+    p->bb = -26.0;
+    p->cc = 24.0;
+    return YK_OK;
+}
+
+const char* yk_last_error(const yk_ctx* ctx)
+{
+    return ctx ? ctx->errmsg.c_str() : g_err_noctx.c_str();
+}
+
+int yk_destroy(yk_ctx* c)
+{
+    if (!c) return YK_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
+    cudaFree(c->x);
+    cudaFree(c->v);
+    cudaFree(c->vold);
+    cudaFree(c->a);
+    cudaFree(c->zii);
+    cudaFree(c->aii);
+    cudaFree(c->pos);
+    cudaFree(c->fpart);
+    cudaFree(c->kpart);
+    cudaFree(c->ds);
+    cudaFree(c->err);
+    cudaFree(c->series);
+    cudaFree(c->series_idx);
+    cudaFreeHost(c->h_ds);
+    cudaFreeHost(c->h_err);
+    cudaFree(c->flush_buf);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return YK_OK;
+}
+
+int yk_create(const yk_params* p, int n, const double* x, const double* v, const double* zii,
+              const double* aii, yk_ctx** out)
+{
+    if (!out) return fail(nullptr, YK_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!p || !x) return fail(nullptr, YK_ERR_ARG, "params and x are required");
+    if (n < 1) return fail(nullptr, YK_ERR_ARG, "n must be >= 1 (got %d)", n);
+    if (n > (1 << 26)) return fail(nullptr, YK_ERR_ARG, "n = %d exceeds 2^26", n);
+    int rc = check_params(p);
+    if (rc) return rc;
+    if ((p->sim_type == YK_SIM_ION_MIXTURE || p->sim_type == YK_SIM_NUCLEON) && !zii)
+        return fail(nullptr, YK_ERR_ARG, "this sim_type needs zii");
+    if (p->sim_type == YK_SIM_ION_MIXTURE && !aii)
+        return fail(nullptr, YK_ERR_ARG, "ion-mixture runs need aii");
+    if (!all_finite(x, 3 * (size_t)n) || (v && !all_finite(v, 3 * (size_t)n)) ||
+        (zii && !all_finite(zii, n)) || (aii && !all_finite(aii, n)))
+        return fail(nullptr, YK_ERR_NONFINITE, "NaN or Inf in an input array");
+    if (aii)
+        for (int i = 0; i < n; ++i)
+            if (!(aii[i] > 0.0)) return fail(nullptr, YK_ERR_ARG, "aii(%d) must be > 0", i);
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(nullptr, YK_ERR_CUDA, "no CUDA device available");
+    if (p->device < 0 || p->device >= ndev)
+        return fail(nullptr, YK_ERR_ARG, "device %d out of range (have %d)", p->device, ndev);
+
+    yk_ctx* c = new yk_ctx();
+    c->p = *p;
+    c->n = n;
+    c->dev = p->device;
+    c->time = p->time;
+    if (cudaSetDevice(c->dev) != cudaSuccess) {
+        delete c;
+        return fail(nullptr, YK_ERR_CUDA, "cudaSetDevice(%d) failed", p->device);
+    }
+    setup_args(c);
+
+    // HBM admission: refuse up front rather than fail half-way.
+    const size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
+                         sizeof(double4) * (size_t)n +
+                         sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        delete c;
+        return fail(nullptr, YK_ERR_CUDA, "cudaMemGetInfo failed");
+    }
+    if (bytes + (64u << 20) > free_b) {
+        delete c;
+        return fail(nullptr, YK_ERR_NOMEM, "needs %zu bytes, %zu free", bytes, free_b);
+    }
+
+#define ALLOC(ptr, cnt)                                                                 \
+    do {                                                                                \
+        if (cudaMalloc((void**)&(ptr), sizeof(*(ptr)) * (size_t)(cnt)) != cudaSuccess) { \
+            yk_destroy(c);                                                              \
+            return fail(nullptr, YK_ERR_NOMEM, "cudaMalloc of " #ptr " failed");        \
+        }                                                                               \
+    } while (0)
+    ALLOC(c->x, 3 * (size_t)n);
+    ALLOC(c->v, 3 * (size_t)n);
+    ALLOC(c->vold, 3 * (size_t)n);
+    ALLOC(c->a, 3 * (size_t)(n + 3));
+    ALLOC(c->zii, n);
+    ALLOC(c->aii, n);
+    ALLOC(c->pos, n);
+    ALLOC(c->fpart, 8 * (size_t)c->nfb);
+    ALLOC(c->kpart, NKIN * (size_t)c->nvb);
+    ALLOC(c->ds, 1);
+    ALLOC(c->err, 1);
+    ALLOC(c->series_idx, 1);
+#undef ALLOC
+    if (cudaMallocHost((void**)&c->h_ds, sizeof(DevScalars)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_err, sizeof(unsigned)) != cudaSuccess) {
+        yk_destroy(c);
+        return fail(nullptr, YK_ERR_NOMEM, "pinned host staging failed");
+    }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        yk_destroy(c);
+        return fail(nullptr, YK_ERR_CUDA, "stream creation failed");
+    }
+    cudaStream_t st = c->stream;
+    std::vector<double> fill(n);
+    cudaMemcpyAsync(c->x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st);
+    if (v) cudaMemcpyAsync(c->v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st);
+    else cudaMemsetAsync(c->v, 0, sizeof(double) * 3 * n, st);
+    cudaMemsetAsync(c->vold, 0, sizeof(double) * 3 * n, st);
+    cudaMemsetAsync(c->a, 0, sizeof(double) * 3 * (n + 3), st);
+    if (zii) {
+        cudaMemcpyAsync(c->zii, zii, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    } else {
+        for (int i = 0; i < n; ++i) fill[i] = p->zi;
+        cudaMemcpyAsync(c->zii, fill.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);
+    }
+    if (aii) {
+        cudaMemcpyAsync(c->aii, aii, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    } else {
+        for (int i = 0; i < n; ++i) fill[i] = p->ai > 0.0 ? p->ai : 1.0;
+        cudaMemcpyAsync(c->aii, fill.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    }
+    cudaMemsetAsync(c->ds, 0, sizeof(DevScalars), st);
+    cudaMemsetAsync(c->err, 0, sizeof(unsigned), st);
+    cudaMemsetAsync(c->series_idx, 0, sizeof(int), st);
+    c->pos_dirty = true;
+    g_launches += enqueue_pack(c);
+    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        yk_destroy(c);
+        return fail(nullptr, YK_ERR_CUDA, "initial upload failed");
+    }
+    *out = c;
+    return YK_OK;
+}
+
+int yk_accel(yk_ctx* c, int do_meas, double* a_out, yk_scalars* out)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    CK(c, cudaSetDevice(c->dev));
+    const bool meas = do_meas != 0;
+    int k = enqueue_pack(c);
+    k += enqueue_force(c, meas);
+    k += enqueue_finish(c, meas, 0, false);
+    g_launches += k;
+    if (a_out)
+        CK(c, cudaMemcpyAsync(a_out, c->a, sizeof(double) * 3 * (size_t)(c->n + 3),
+                              cudaMemcpyDeviceToHost, c->stream));
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    fill_scalars(c, out);
+    return YK_OK;
+}
+
+int yk_newton(yk_ctx* c, int do_meas, yk_scalars* out)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    CK(c, cudaSetDevice(c->dev));
+    int k = enqueue_pack(c);
+    k += enqueue_newton(c, do_meas != 0, false);
+    g_launches += k;
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    c->time = c->time + c->p.dt;            // vel_verlet_2.f:114
+    fill_scalars(c, out);
+    return YK_OK;
+}
+
+static int finish_run(yk_ctx* c, int nsteps, bool want_series, yk_scalars* series);
+
+static int capture_graph(yk_ctx* c, int K, int me, bool series)
+{
+    drop_graph(c);
+    cudaGraph_t g = nullptr;
+    CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int kernels = 0;
+    for (int s = 1; s <= K; ++s) kernels += enqueue_newton(c, me > 0 && s % me == 0, series);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) return fail(c, YK_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        c->graph = nullptr;
+        return fail(c, YK_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    }
+    c->graph_K = K;
+    c->graph_me = me;
+    c->graph_series = series ? 1 : 0;
+    c->graph_kernels = kernels;
+    return YK_OK;
+}
+
+int yk_run(yk_ctx* c, int nsteps, int meas_every, yk_scalars* series)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    if (nsteps < 0 || meas_every < 0) return fail(c, YK_ERR_ARG, "nsteps and meas_every must be >= 0");
+    if (nsteps == 0) return YK_OK;
+    CK(c, cudaSetDevice(c->dev));
+    const bool want_series = series != nullptr;
+    if (want_series && c->series_cap < nsteps) {
+        drop_graph(c);
+        cudaFree(c->series);
+        c->series = nullptr;
+        c->series_cap = 0;
+        CK(c, cudaMalloc((void**)&c->series, sizeof(double) * 13 * (size_t)nsteps));
+        c->series_cap = nsteps;
+    }
+    CK(c, cudaMemsetAsync(c->series_idx, 0, sizeof(int), c->stream));
+    int k = enqueue_pack(c);
+    if (c->perf_on) {
+        // Timed path: step by step, event pairs around every force kernel.
+        c->ev_used = 0;
+        cudaEvent_t e0 = next_event(c), e1 = next_event(c);
+        CK(c, cudaEventRecord(e0, c->stream));
+        for (int s = 1; s <= nsteps; ++s) {
+            if (c->flush_bytes)
+                CK(c, cudaMemsetAsync(c->flush_buf, s & 0xff, c->flush_bytes, c->stream));
+            k += enqueue_newton(c, meas_every > 0 && s % meas_every == 0, want_series, true);
+        }
+        CK(c, cudaEventRecord(e1, c->stream));
+        g_launches += k;
+        int rc = sync_and_check(c);
+        if (rc) return rc;
+        float ms = 0.f;
+        CK(c, cudaEventElapsedTime(&ms, e0, e1));
+        c->perf.run_ms += ms;
+        for (int q = 2; q + 1 < c->ev_used; q += 2) {
+            CK(c, cudaEventElapsedTime(&ms, c->ev_pool[q], c->ev_pool[q + 1]));
+            c->perf.force_ms += ms;
+            c->perf.force_calls += 1;
+        }
+        c->perf.steps += nsteps;
+        return finish_run(c, nsteps, want_series, series);
+    }
+    // K steps per graph: a multiple of meas_every near 50 so that every
+    // launch of the graph has the same measuring pattern.
+    int K = 50;
+    if (meas_every > 0) K = meas_every * ((50 + meas_every - 1) / meas_every);
+    if (K > nsteps) K = 0;
+    int done = 0;
+    if (K > 0) {
+        if (!(c->graph && c->graph_K == K && c->graph_me == meas_every &&
+              c->graph_series == (want_series ? 1 : 0))) {
+            int rc = capture_graph(c, K, meas_every, want_series);
+            if (rc) return rc;
+        }
+        while (done + K <= nsteps) {
+            CK(c, cudaGraphLaunch(c->graph, c->stream));
+            k += c->graph_kernels;
+            done += K;
+        }
+    }
+    for (int s = done + 1; s <= nsteps; ++s)
+        k += enqueue_newton(c, meas_every > 0 && s % meas_every == 0, want_series);
+    g_launches += k;
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    return finish_run(c, nsteps, want_series, series);
+}
+
+static int finish_run(yk_ctx* c, int nsteps, bool want_series, yk_scalars* series)
+{
+    if (want_series) {
+        std::vector<double> h(13 * (size_t)nsteps);
+        CK(c, cudaMemcpy(h.data(), c->series, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < nsteps; ++s) {
+            const double* o = &h[13 * (size_t)s];
+            c->time = c->time + c->p.dt;
+            series[s].ev = o[0];
+            series[s].vir = o[1];
+            series[s].px = o[2];
+            series[s].ek = o[3];
+            for (int q = 0; q < 9; ++q) series[s].pp[q] = o[4 + q];
+            series[s].time = c->time;
+        }
+    } else {
+        for (int s = 0; s < nsteps; ++s) c->time = c->time + c->p.dt;
+    }
+    return YK_OK;
+}
+
+int yk_get_state(yk_ctx* c, double* x, double* v, double* vold, double* a)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    CK(c, cudaSetDevice(c->dev));
+    const size_t b = sizeof(double) * 3 * (size_t)c->n;
+    if (x) CK(c, cudaMemcpyAsync(x, c->x, b, cudaMemcpyDeviceToHost, c->stream));
+    if (v) CK(c, cudaMemcpyAsync(v, c->v, b, cudaMemcpyDeviceToHost, c->stream));
+    if (vold) CK(c, cudaMemcpyAsync(vold, c->vold, b, cudaMemcpyDeviceToHost, c->stream));
+    if (a) CK(c, cudaMemcpyAsync(a, c->a, b, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return YK_OK;
+}
+
+int yk_set_state(yk_ctx* c, const double* x, const double* v, const double* vold, const double* a)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    const size_t cnt = 3 * (size_t)c->n;
+    if ((x && !all_finite(x, cnt)) || (v && !all_finite(v, cnt)) || (vold && !all_finite(vold, cnt)) ||
+        (a && !all_finite(a, cnt)))
+        return fail(c, YK_ERR_NONFINITE, "NaN or Inf in a state array");
+    CK(c, cudaSetDevice(c->dev));
+    const size_t b = sizeof(double) * cnt;
+    if (x) CK(c, cudaMemcpyAsync(c->x, x, b, cudaMemcpyHostToDevice, c->stream));
+    if (v) CK(c, cudaMemcpyAsync(c->v, v, b, cudaMemcpyHostToDevice, c->stream));
+    if (vold) CK(c, cudaMemcpyAsync(c->vold, vold, b, cudaMemcpyHostToDevice, c->stream));
+    if (a) CK(c, cudaMemcpyAsync(c->a, a, b, cudaMemcpyHostToDevice, c->stream));
+    if (x) {
+        c->pos_dirty = true;
+        g_launches += enqueue_pack(c);
+    }
+    CK(c, cudaStreamSynchronize(c->stream));
+    return YK_OK;
+}
+
+int yk_set_box(yk_ctx* c, const double xl[3])
+{
+    if (!c || !xl) return fail(c, YK_ERR_ARG, "ctx and xl are required");
+    for (int k = 0; k < 3; ++k)
+        if (!(xl[k] > 0.0) || !std::isfinite(xl[k])) return fail(c, YK_ERR_ARG, "xl must be > 0");
+    for (int k = 0; k < 3; ++k) c->p.xl[k] = xl[k];
+    setup_args(c);
+    drop_graph(c);
+    return YK_OK;
+}
+
+int yk_perf_enable(yk_ctx* c, int enable, size_t flush_bytes)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    CK(c, cudaSetDevice(c->dev));
+    c->perf_on = enable != 0;
+    c->perf = yk_perf{};
+    if (flush_bytes != c->flush_bytes) {
+        cudaFree(c->flush_buf);
+        c->flush_buf = nullptr;
+        c->flush_bytes = 0;
+        if (flush_bytes) {
+            CK(c, cudaMalloc((void**)&c->flush_buf, flush_bytes));
+            c->flush_bytes = flush_bytes;
+        }
+    }
+    return YK_OK;
+}
+
+int yk_perf_read(yk_ctx* c, yk_perf* out)
+{
+    if (!c || !out) return fail(c, YK_ERR_ARG, "ctx and out are required");
+    *out = c->perf;
+    return YK_OK;
+}
+
+int yk_peak_probe(int device, int kind, double* tflops)
+{
+    if (!tflops || (kind != 0 && kind != 1)) return fail(nullptr, YK_ERR_ARG, "bad peak probe arguments");
+    if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, YK_ERR_CUDA, "cudaSetDevice failed");
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int blocks = sms * 8, threads = 256, iters = 1 << 13;
+    void* out = nullptr;
+    if (cudaMalloc(&out, sizeof(double) * blocks * threads) != cudaSuccess)
+        return fail(nullptr, YK_ERR_NOMEM, "probe buffer");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 7; ++rep) {
+        cudaEventRecord(e0);
+        if (kind == 0) k_fma_probe<double><<<blocks, threads>>>((double*)out, iters, 0.9999999, 1e-7);
+        else k_fma_probe<float><<<blocks, threads>>>((float*)out, iters, 0.9999999f, 1e-7f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep >= 2 && ms < best) best = ms;
+    }
+    g_launches += 7;
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess) return fail(nullptr, YK_ERR_CUDA, "probe: %s", cudaGetErrorString(e));
+    const double fmas = (double)blocks * threads * iters * PROBE_CHAINS;
+    *tflops = 2.0 * fmas / (best * 1e-3) / 1e12;
+    return YK_OK;
+}
+
+int yk_host_register(void* ptr, size_t bytes)
+{
+    if (!ptr || !bytes) return YK_ERR_ARG;
+    cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+    if (e != cudaSuccess) return fail(nullptr, YK_ERR_CUDA, "cudaHostRegister: %s", cudaGetErrorString(e));
+    return YK_OK;
+}
+
+int yk_host_unregister(void* ptr)
+{
+    if (!ptr) return YK_ERR_ARG;
+    cudaError_t e = cudaHostUnregister(ptr);
+    if (e != cudaSuccess) return fail(nullptr, YK_ERR_CUDA, "cudaHostUnregister: %s", cudaGetErrorString(e));
+    return YK_OK;
+}
+
+}  // extern "C"

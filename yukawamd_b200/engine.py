@@ -1,0 +1,169 @@
+"""Host-side mirror of the reference's force-call and integrator interface.
+
+The Fortran code calls two argument-less routines that work on module
+globals (md_globals.f:153-172):
+
+    call accel(do_measurements)     ! int_control.f:52-81
+    call newton(do_measurements)    ! vel_verlet_2.f:18-120
+
+Engine keeps the same shape: the particle arrays live on the device, the
+scalar results (ev, vir, px, ek, pp, time) come back as attributes after each
+call, and errors raise EngineError carrying the C-ABI status, the way the
+Fortran shim maps them to md_exit.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import check, lib
+
+_dp = C.POINTER(C.c_double)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("arrays must be C-contiguous float64")
+    return a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+
+
+class Engine:
+    """One simulation box on one GPU.
+
+    params: abi.YkParams (or a configs.Workload, whose arrays are then used
+    when x is None).  x, v: double[3n] in the Fortran layout x(3,0:n-1).
+    """
+
+    def __init__(self, params, x=None, v=None, zii=None, aii=None, **overrides):
+        if not isinstance(params, abi.YkParams):
+            w = params
+            params = w.yk_params(**overrides)
+            x = w.x if x is None else x
+            v = w.v if v is None else v
+            zii = w.zii if zii is None else zii
+            aii = w.aii if aii is None else aii
+        else:
+            for k, val in overrides.items():
+                setattr(params, k, val)
+        self.params = params
+        x, v, zii, aii = _f64(x), _f64(v), _f64(zii), _f64(aii)
+        if x is None:
+            raise ValueError("positions are required")
+        self.n = len(x) // 3
+        self._lib = lib()
+        self._ctx = C.c_void_p()
+        check(self._lib.yk_create(C.byref(params), self.n, _ptr(x), _ptr(v), _ptr(zii),
+                                  _ptr(aii), C.byref(self._ctx)))
+        self.scalars = abi.YkScalars()
+        self.a = np.zeros(3 * (self.n + 3))
+
+    # -- the reference's two entry points ---------------------------------
+    def accel(self, do_measurements=True, fetch_a=True):
+        """accel(do_measurements): forces from the device-resident positions.
+        Fills self.a (double[3(n+3)], the reference layout) when fetch_a."""
+        check(self._lib.yk_accel(self._ctx, int(bool(do_measurements)),
+                                 _ptr(self.a) if fetch_a else None,
+                                 C.byref(self.scalars)), self._ctx)
+        return self.scalars
+
+    def newton(self, do_measurements=False):
+        """newton(do_measurements): one integrator step on the device."""
+        check(self._lib.yk_newton(self._ctx, int(bool(do_measurements)),
+                                  C.byref(self.scalars)), self._ctx)
+        return self.scalars
+
+    # -- device-resident stepping ---------------------------------------
+    def run(self, nsteps, meas_every=0, series=True):
+        """nsteps steps launched as CUDA graphs; returns the per-step scalars
+        (a ctypes array of YkScalars) when series, else None."""
+        buf = (abi.YkScalars * nsteps)() if series and nsteps > 0 else None
+        check(self._lib.yk_run(self._ctx, int(nsteps), int(meas_every),
+                               buf if buf is not None else None), self._ctx)
+        if buf is not None and nsteps > 0:
+            self.scalars = buf[nsteps - 1]
+        return buf
+
+    # -- sync points ------------------------------------------------------
+    def get_state(self):
+        n3 = 3 * self.n
+        x, v, vold, a = (np.empty(n3) for _ in range(4))
+        check(self._lib.yk_get_state(self._ctx, _ptr(x), _ptr(v), _ptr(vold), _ptr(a)),
+              self._ctx)
+        return x, v, vold, a
+
+    def get_into(self, x=None, v=None, vold=None, a=None):
+        check(self._lib.yk_get_state(self._ctx, _ptr(x), _ptr(v), _ptr(vold), _ptr(a)),
+              self._ctx)
+
+    def set_state(self, x=None, v=None, vold=None, a=None):
+        x, v, vold, a = _f64(x), _f64(v), _f64(vold), _f64(a)
+        if a is not None and len(a) == 3 * (self.n + 3):
+            a = np.ascontiguousarray(a[:3 * self.n])
+        check(self._lib.yk_set_state(self._ctx, _ptr(x), _ptr(v), _ptr(vold), _ptr(a)),
+              self._ctx)
+
+    def set_box(self, xl):
+        arr = (C.c_double * 3)(*[float(t) for t in xl])
+        check(self._lib.yk_set_box(self._ctx, C.cast(arr, _dp)), self._ctx)
+        for k in range(3):
+            self.params.xl[k] = float(xl[k])
+
+    # -- timers (the reference's perf.f newton / accel timers) --------------
+    def perf_enable(self, enable=True, flush_bytes=0):
+        check(self._lib.yk_perf_enable(self._ctx, int(bool(enable)), int(flush_bytes)),
+              self._ctx)
+
+    def perf_read(self):
+        out = abi.YkPerf()
+        check(self._lib.yk_perf_read(self._ctx, C.byref(out)), self._ctx)
+        return out
+
+    @property
+    def time(self):
+        return self.scalars.time
+
+    def close(self):
+        if self._ctx:
+            self._lib.yk_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kernel_launch_count():
+    return int(lib().yk_kernel_launch_count())
+
+
+def peak_probe(device=0, kind=0):
+    """Measured FMA throughput of the GPU in TFLOP/s (kind 0 FP64, 1 FP32)."""
+    out = C.c_double()
+    check(lib().yk_peak_probe(int(device), int(kind), C.byref(out)))
+    return out.value
+
+
+def version():
+    return lib().yk_version().decode()
+
+
+def host_register(arr):
+    check(lib().yk_host_register(arr.ctypes.data_as(C.c_void_p), arr.nbytes))
+
+
+def host_unregister(arr):
+    check(lib().yk_host_unregister(arr.ctypes.data_as(C.c_void_p)))
