@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--meas-every", type=int, default=10)
     ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--n", type=int, default=0,
+                    help="override the particle count (same density; for profiling runs)")
     ap.add_argument("--no-companion", action="store_true",
                     help="skip the mixed-precision companion measurement")
     ap.add_argument("--no-e2e", action="store_true")
@@ -64,13 +66,14 @@ def parse():
     return ap.parse_args()
 
 
-def make_workload(kind, seed):
+def make_workload(kind, seed, n=0):
     from yukawamd_b200 import configs
+    kw = {"n": n} if n else {}
     if kind == "mix":
-        return configs.ion_mixture_cfg(seed)
+        return configs.ion_mixture_cfg(seed, **kw)
     if kind == "ocp":
-        return configs.pure_ion_ocp(seed)
-    return configs.nucleon_matter(seed)
+        return configs.pure_ion_ocp(seed, **kw)
+    return configs.nucleon_matter(seed, **kw)
 
 
 def workload_desc(w, kind):
@@ -302,7 +305,7 @@ def run_ours(args, dist):
     from yukawamd_b200 import _lib
     from yukawamd_b200.engine import peak_probe
     kind = args.workload
-    w = make_workload(kind, args.seed + dist.rank)
+    w = make_workload(kind, args.seed + dist.rank, args.n)
     pairs_step = w.pairs_per_step
     K, W, me = args.steps, args.warmup, args.meas_every
 
@@ -388,7 +391,7 @@ def run_reference(args):
     """The reference's CPU algorithm (OpenMP C restatement) on all host cores."""
     from oracle.oracle import Oracle
     kind = args.workload
-    w = make_workload(kind, args.seed)
+    w = make_workload(kind, args.seed, args.n)
     n = w.n
     p = w.yk_params()
     cores = os.cpu_count() or 1

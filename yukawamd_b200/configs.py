@@ -61,7 +61,8 @@ def cancel_vcom_tnorm(v, aii, kT, xmass=abi.XMASS):
     vcom = (aii[:, None] * v).sum(0) / aii.sum()
     v = v - vcom
     eka = 0.5 * xmass * float((aii * (v * v).sum(1)).sum()) / len(aii)
-    v = v / math.sqrt(eka / (1.5 * kT))
+    if eka > 0.0:                   # a single particle has no thermal motion left
+        v = v / math.sqrt(eka / (1.5 * kT))
     return v.reshape(-1)
 
 
