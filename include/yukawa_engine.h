@@ -170,6 +170,22 @@ YK_API int yk_set_state(yk_ctx* ctx, const double* x, const double* v,
 YK_API int yk_set_box(yk_ctx* ctx, const double xl[3]);
 
 /*
+ * Engine tunables (not reference parameters): which force kernel runs and
+ * how its work is cut.  yk_create picks defaults; the autotuner
+ * (yukawamd_b200/tune.py) measures the alternatives and sets them here.
+ */
+typedef struct yk_tuning {
+    int force_kernel;     /* 0 auto, 1 row kernel (each pair from both sides),
+                             2 half-pair kernel (Newton's third law, scratch)  */
+    int pair_seg;         /* source tiles per job of the half-pair kernel     */
+    int sort_every;       /* steps between Morton re-orderings (-1 = never)   */
+    int graph_steps;      /* steps captured per CUDA graph by yk_run          */
+} yk_tuning;
+
+YK_API int yk_get_tuning(yk_ctx* ctx, yk_tuning* out);
+YK_API int yk_set_tuning(yk_ctx* ctx, const yk_tuning* t);
+
+/*
  * Timers, the counterpart of the reference's perf.f report (perf.f:60-178:
  * 'newton', 'accel' and 'calc_a' wall-clock timers).  With yk_perf_enable(ctx,
  * 1, flush_bytes) the following yk_run calls launch step by step (no graph)

@@ -39,10 +39,12 @@ def workload(kind, n, seed):
     return configs.nucleon_matter(seed, n)
 
 
-def check_accel(orc, w, prec, meas, mix_mode=abi.YK_MIX_COMPAT, gpu=None):
+def check_accel(orc, w, prec, meas, mix_mode=abi.YK_MIX_COMPAT, tuning=None):
     p = w.yk_params(precision=prec, mix_mode=mix_mode)
     n = w.n
     with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        if tuning:
+            e.set_tuning(**tuning)
         s = e.accel(meas)
         a_gpu = e.a.copy()
     a_ref, s_ref = orc.accel(p, w.x, w.zii, w.aii, meas)
@@ -62,24 +64,33 @@ def check_accel(orc, w, prec, meas, mix_mode=abi.YK_MIX_COMPAT, gpu=None):
         assert s.ev == 0.0 and s.px == 0.0 and all(t == 0.0 for t in s.pp)
 
 
+KERNELS = {"rows": dict(force_kernel=abi.KERNEL_ROWS),
+           "pairs": dict(force_kernel=abi.KERNEL_PAIRS),
+           "pairs-unsorted-seg3": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, pair_seg=3)}
+
+
+@pytest.mark.parametrize("kern", list(KERNELS))
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
 @pytest.mark.parametrize("meas", [True, False], ids=["meas", "force"])
 @pytest.mark.parametrize("kind,n", [("pure", 4096), ("mix", 3000), ("nn", 3000)])
-def test_accel_matches_oracle(gpu, orc, kind, n, meas, prec):
-    check_accel(orc, workload(kind, n, 100 + n), prec, meas)
+def test_accel_matches_oracle(gpu, orc, kind, n, meas, prec, kern):
+    check_accel(orc, workload(kind, n, 100 + n), prec, meas, tuning=KERNELS[kern])
 
 
+@pytest.mark.parametrize("kern", ["rows", "pairs"])
 @pytest.mark.parametrize("n", [1, 2, 3, 17, 127, 128, 129, 255, 257])
 @pytest.mark.parametrize("kind", ["pure", "mix", "nn"])
-def test_ragged_sizes(gpu, orc, kind, n):
+def test_ragged_sizes(gpu, orc, kind, n, kern):
     w = workload(kind, n, 7 + n)
-    check_accel(orc, w, abi.YK_PREC_FP64, True)
-    check_accel(orc, w, abi.YK_PREC_FP64, False)
+    check_accel(orc, w, abi.YK_PREC_FP64, True, tuning=KERNELS[kern])
+    check_accel(orc, w, abi.YK_PREC_FP64, False, tuning=KERNELS[kern])
 
 
+@pytest.mark.parametrize("kern", ["rows", "pairs"])
 @pytest.mark.parametrize("mode", [abi.YK_MIX_COMPAT, abi.YK_MIX_FIXED], ids=["compat", "fixed"])
-def test_mix_last_particle_mode(gpu, orc, mode):
-    check_accel(orc, workload("mix", 513, 5), abi.YK_PREC_FP64, False, mix_mode=mode)
+def test_mix_last_particle_mode(gpu, orc, mode, kern):
+    check_accel(orc, workload("mix", 513, 5), abi.YK_PREC_FP64, False, mix_mode=mode,
+                tuning=KERNELS[kern])
 
 
 def test_known_answers_through_capi(gpu):
@@ -156,23 +167,32 @@ def test_newton_steps_match_oracle(gpu, orc, kind):
     assert rel(s.px, s_ref.px) <= 1e-11
 
 
+@pytest.mark.parametrize("kern", ["rows", "pairs"])
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
-def test_run_graph_equals_newton_loop(gpu, prec):
-    """yk_run (CUDA graphs) is bit-identical to the same steps via yk_newton."""
+def test_run_graph_equals_newton_loop(gpu, prec, kern):
+    """yk_run (CUDA graphs, Morton re-sorts inside) is bit-identical to the
+    same steps via yk_newton."""
     w = configs.pure_ion_ocp(51, 2000)
     p = w.yk_params(precision=prec)
-    steps, me = 57, 5
+    steps, me = 157, 5
     with Engine(p, w.x, w.v, w.zii, w.aii) as e1:
+        e1.set_tuning(**KERNELS[kern])
         e1.accel(True)
-        ser1 = [abi.YkScalars.from_buffer_copy(e1.newton((k + 1) % me == 0)) for k in range(steps)]
+        # global step g (1-based) measures when g > 3 and (g - 3) % me == 0,
+        # which is the pattern of the two yk_run calls below
+        ser1 = [abi.YkScalars.from_buffer_copy(e1.newton(g > 3 and (g - 3) % me == 0))
+                for g in range(1, steps + 1)]
         st1 = e1.get_state()
     with Engine(p, w.x, w.v, w.zii, w.aii) as e2:
+        e2.set_tuning(**KERNELS[kern])
         e2.accel(True)
-        ser2 = e2.run(steps, me)
+        e2.run(3, me, series=False)          # start unaligned with the sort cadence
+        ser2 = e2.run(steps - 3, me)
         st2 = e2.get_state()
     for A, B in zip(st1, st2):
         assert np.array_equal(A, B)
-    for s1, s2 in zip(ser1, ser2):
+    assert len(ser2) == steps - 3
+    for s1, s2 in zip(ser1[3:], ser2):
         assert bytes(s1) == bytes(s2)
 
 

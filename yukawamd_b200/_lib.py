@@ -31,6 +31,8 @@ SIGNATURES = {
     "yk_get_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_box": (C.c_int, [_ctx, _dp]),
+    "yk_get_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
+    "yk_set_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_perf_enable": (C.c_int, [_ctx, C.c_int, C.c_size_t]),
     "yk_perf_read": (C.c_int, [_ctx, C.POINTER(abi.YkPerf)]),
     "yk_peak_probe": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),

@@ -106,6 +106,20 @@ class YkScalars(C.Structure):
                 "pp": list(self.pp), "time": self.time}
 
 
+class YkTuning(C.Structure):
+    _fields_ = [
+        ("force_kernel", C.c_int),
+        ("pair_seg", C.c_int),
+        ("sort_every", C.c_int),
+        ("graph_steps", C.c_int),
+    ]
+
+
+KERNEL_AUTO = 0
+KERNEL_ROWS = 1
+KERNEL_PAIRS = 2
+
+
 class YkPerf(C.Structure):
     _fields_ = [
         ("run_ms", C.c_double),

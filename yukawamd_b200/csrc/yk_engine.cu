@@ -1,12 +1,14 @@
 // yk_engine.cu -- the C-ABI of include/yukawa_engine.h.
 //
 // One yk_ctx per simulation box.  Device state stays resident between calls:
-// x, v, vold, a (Fortran layout), zii, aii, the packed double4 positions the
-// force kernels stream, per-CTA partial sums and the md_globals scalars.
+// x, v, vold, a in the caller's (Fortran) layout and order, zii, aii, the
+// Morton-ordered double4 positions the force kernels stream, the permutation
+// between the two orders, scratch partial sums and the md_globals scalars.
 // Every call runs on the context's own stream; calls that return results to
 // the host synchronise that stream once at the end.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -15,13 +17,20 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "../../include/yukawa_engine.h"
 #include "yk_force.cuh"
+#include "yk_pairs.cuh"
+#include "yk_sort.cuh"
 #include "yk_verlet.cuh"
 
 using namespace yk;
 
 static std::atomic<unsigned long long> g_launches{0};
+static thread_local std::string g_err_noctx;
+
+#define YK_VERSION_STR "yukawamd_b200 0.2.0 (sm_100a)"
 
 // FMA-throughput probe: PROBE_CHAINS independent dependent chains per thread.
 constexpr int PROBE_CHAINS = 8;
@@ -40,42 +49,74 @@ __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b)
     for (int q = 0; q < PROBE_CHAINS; ++q) s += x[q];
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
-static thread_local std::string g_err_noctx;
 
-#define YK_VERSION_STR "yukawamd_b200 0.1.0 (sm_100a)"
+// Largest scratch the half-pair kernel may take before auto mode falls back
+// to the scratch-free row kernel.
+constexpr size_t PAIR_SCRATCH_BUDGET = size_t(8) << 30;
+constexpr int DEFAULT_SEG = 8;
+constexpr int DEFAULT_SORT_EVERY = 50;
+constexpr int DEFAULT_GRAPH_STEPS = 50;
+constexpr int MAX_GRAPHS = 8;
+
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    int K = 0, me = 0, phase = 0, series = 0, kernels = 0;
+    unsigned long long stamp = 0;
+};
 
 struct yk_ctx {
     yk_params p;
     int n = 0;
     int dev = 0;
     cudaStream_t stream = nullptr;
+    // state in the caller's order and layout
     double *x = nullptr, *v = nullptr, *vold = nullptr, *a = nullptr;
     double *zii = nullptr, *aii = nullptr;
+    // Morton order
     double4* pos = nullptr;
+    int *perm = nullptr, *iperm = nullptr;
+    unsigned *keys0 = nullptr, *keys1 = nullptr;
+    int* idx0 = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    // reductions and outputs
     double *fpart = nullptr, *kpart = nullptr;
     DevScalars* ds = nullptr;
     unsigned* err = nullptr;
     double* series = nullptr;
     int series_cap = 0;
     int* series_idx = nullptr;
-    DevScalars* h_ds = nullptr;     // pinned staging for scalars + error word
+    DevScalars* h_ds = nullptr;
     unsigned* h_err = nullptr;
+    // half-pair kernel
+    double *Si = nullptr, *Sj = nullptr, *Sm = nullptr;
+    int2* jobs = nullptr;
+    int* job_counter = nullptr;
+    PairJobs pj{};
+    // argument blocks and tunables
     ForceArgs fa{};
     StepArgs sa{};
     FinishArgs fz_base{};
     int nfb = 0, nvb = 0;
+    int kernel = 2;                 // 1 rows, 2 pairs (resolved, never 0)
+    int kernel_req = 0;             // as requested (0 = auto)
+    int seg = DEFAULT_SEG;
+    int sort_every = DEFAULT_SORT_EVERY;
+    int graph_steps = DEFAULT_GRAPH_STEPS;
+    long long step_count = 0;       // integrator steps since create
     double time = 0.0;
-    bool pos_dirty = true;
-    // perf timers (yk_perf_enable)
+    bool pos_dirty = true;          // positions changed on the host: repack
+    bool need_sort = true;
+    // timers
     bool perf_on = false;
     size_t flush_bytes = 0;
     unsigned char* flush_buf = nullptr;
     std::vector<cudaEvent_t> ev_pool;
     int ev_used = 0;
     yk_perf perf{};
-    // cached K-step graph
-    cudaGraphExec_t graph = nullptr;
-    int graph_K = 0, graph_me = -1, graph_series = -1, graph_kernels = 0;
+    // cached K-step graphs
+    std::vector<GraphEntry> graphs;
+    unsigned long long graph_clock = 0;
     std::string errmsg;
 };
 
@@ -171,7 +212,6 @@ static void setup_args(yk_ctx* c)
     FinishArgs& z = c->fz_base;
     z = FinishArgs{};
     z.n = c->n;
-    z.half = 0.5;
     z.coef = f.coef;
     z.rho = p.rho;
     z.kT = p.kT;
@@ -184,38 +224,88 @@ static void setup_args(yk_ctx* c)
     c->nvb = (c->n + VBLOCK - 1) / VBLOCK;
 }
 
-static void drop_graph(yk_ctx* c)
+static void drop_graphs(yk_ctx* c)
 {
-    if (c->graph) cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-    c->graph_K = 0;
-    c->graph_me = -1;
-    c->graph_series = -1;
-    c->graph_kernels = 0;
+    for (auto& g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+}
+
+// Scratch bytes of the half-pair kernel for n particles and segment length.
+static size_t pair_scratch_bytes(int n, int seg)
+{
+    const size_t M = (size_t)(n + PB - 1) / PB;
+    const size_t nseg = (M + seg - 1) / seg;
+    const size_t units = M * (M + 1) / 2;
+    size_t jobs = 0;
+    for (size_t R = 0; R < M; ++R) jobs += (M - R + seg - 1) / seg;
+    return sizeof(double) * (units * PB * 3 + M * nseg * PB * 3 + jobs * NSCAL) + sizeof(int2) * jobs;
+}
+
+static void free_pairs(yk_ctx* c)
+{
+    cudaFree(c->Si);
+    cudaFree(c->Sj);
+    cudaFree(c->Sm);
+    cudaFree(c->jobs);
+    c->Si = c->Sj = c->Sm = nullptr;
+    c->jobs = nullptr;
+    c->pj = PairJobs{};
+}
+
+// Build the job table of the half-pair kernel (costliest jobs first) and its
+// scratch.  Unused Sj / Si slots are never read.
+static int setup_pairs(yk_ctx* c)
+{
+    free_pairs(c);
+    const int M = (c->n + PB - 1) / PB;
+    const int seg = c->seg;
+    std::vector<int2> jobs;
+    std::vector<int> cost;
+    for (int R = 0; R < M; ++R) {
+        const int L = M - R;
+        for (int s = 0; s * seg < L; ++s) {
+            jobs.push_back(make_int2(R, s));
+            const int tiles = std::min(seg, L - s * seg);
+            cost.push_back(2 * tiles - (s == 0 ? 1 : 0));   // diagonal tile ~ half
+        }
+    }
+    std::vector<int> order(jobs.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+    std::stable_sort(order.begin(), order.end(), [&](int u, int w) { return cost[u] > cost[w]; });
+    std::vector<int2> sorted(jobs.size());
+    for (size_t k = 0; k < order.size(); ++k) sorted[k] = jobs[order[k]];
+    const int nseg = (M + seg - 1) / seg;
+    const size_t units = (size_t)M * (M + 1) / 2;
+    CK(c, cudaMalloc((void**)&c->Sj, sizeof(double) * units * PB * 3));
+    CK(c, cudaMalloc((void**)&c->Si, sizeof(double) * (size_t)M * nseg * PB * 3));
+    CK(c, cudaMalloc((void**)&c->Sm, sizeof(double) * sorted.size() * NSCAL));
+    CK(c, cudaMalloc((void**)&c->jobs, sizeof(int2) * sorted.size()));
+    CK(c, cudaMemcpy(c->jobs, sorted.data(), sizeof(int2) * sorted.size(), cudaMemcpyHostToDevice));
+    c->pj.jobs = c->jobs;
+    c->pj.njobs = (int)sorted.size();
+    c->pj.M = M;
+    c->pj.seg = seg;
+    c->pj.nseg_max = nseg;
+    return YK_OK;
+}
+
+static int resolve_kernel(yk_ctx* c)
+{
+    int k = c->kernel_req;
+    if (k == 0) k = (pair_scratch_bytes(c->n, c->seg) <= PAIR_SCRATCH_BUDGET) ? 2 : 1;
+    if (k == 2) {
+        int rc = setup_pairs(c);
+        if (rc) return rc;
+    } else {
+        free_pairs(c);
+    }
+    c->kernel = k;
+    return YK_OK;
 }
 
 // ---------------------------------------------------------------------------
 // launch helpers (all on c->stream; they only enqueue)
-
-template <int SIM, int PREC, bool MEAS>
-static void launch_force_t(yk_ctx* c)
-{
-    k_force_rows<SIM, PREC, MEAS><<<c->nfb, FBLOCK, FORCE_SMEM, c->stream>>>(
-        c->pos, c->aii, c->fa, c->a, c->fpart, c->err);
-}
-
-template <int SIM>
-static void launch_force_s(yk_ctx* c, bool meas)
-{
-    const bool mixed = c->p.precision == YK_PREC_MIXED;
-    if (mixed) {
-        if (meas) launch_force_t<SIM, PREC_MIXED, true>(c);
-        else launch_force_t<SIM, PREC_MIXED, false>(c);
-    } else {
-        if (meas) launch_force_t<SIM, PREC_FP64, true>(c);
-        else launch_force_t<SIM, PREC_FP64, false>(c);
-    }
-}
 
 static cudaEvent_t next_event(yk_ctx* c)
 {
@@ -227,10 +317,77 @@ static cudaEvent_t next_event(yk_ctx* c)
     return c->ev_pool[c->ev_used++];
 }
 
-static int enqueue_force_body(yk_ctx* c, bool meas);
+// Morton sort (full) or repack with the current order (sort = false).
+static int enqueue_order(yk_ctx* c, bool sort)
+{
+    const int n = c->n, nb = c->nvb;
+    cudaStream_t st = c->stream;
+    int k = 0;
+    if (sort) {
+        if (c->sort_every < 0) {
+            // fixed identity order
+            k_morton<<<nb, VBLOCK, 0, st>>>(c->x, n, 0.0, 0.0, 0.0, c->keys0, c->perm);
+        } else {
+            k_morton<<<nb, VBLOCK, 0, st>>>(c->x, n, 1024.0 / c->p.xl[0], 1024.0 / c->p.xl[1],
+                                            1024.0 / c->p.xl[2], c->keys0, c->idx0);
+            size_t bytes = c->cub_bytes;
+            cub::DeviceRadixSort::SortPairs(c->cub_tmp, bytes, c->keys0, c->keys1, c->idx0, c->perm, n,
+                                            0, 30, st);
+        }
+        ++k;
+        c->need_sort = false;
+    }
+    k_apply_perm<<<nb, VBLOCK, 0, st>>>(c->perm, c->iperm, c->x, c->zii, c->pos, n, c->sa.pack_w);
+    c->pos_dirty = false;
+    return k + 1;
+}
+
+template <int SIM, int PREC, bool MEAS>
+static int launch_force_t(yk_ctx* c)
+{
+    if (c->kernel == 1) {
+        k_force_rows<SIM, PREC, MEAS><<<c->nfb, FBLOCK, FORCE_SMEM, c->stream>>>(
+            c->pos, c->perm, c->aii, c->fa, c->a, c->fpart, c->err);
+        return 1;
+    }
+    static int grid = 0;
+    if (grid == 0) {
+        int per_sm = 0, sms = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs<SIM, PREC, MEAS>, PB, 0);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+        grid = std::max(1, per_sm) * std::max(1, sms);
+    }
+    cudaMemsetAsync(c->job_counter, 0, sizeof(int), c->stream);
+    const int g = std::min(grid, c->pj.njobs);
+    k_force_pairs<SIM, PREC, MEAS><<<g, PB, 0, c->stream>>>(c->pos, c->pj, c->job_counter, c->fa,
+                                                            c->Si, c->Sj, c->Sm, c->err);
+    k_combine<SIM><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->Si, c->Sj, c->pj, c->perm, c->zii,
+                                                              c->aii, c->fa, c->a);
+    return 2;
+}
+
+template <int SIM>
+static int launch_force_s(yk_ctx* c, bool meas)
+{
+    if (c->p.precision == YK_PREC_MIXED)
+        return meas ? launch_force_t<SIM, PREC_MIXED, true>(c) : launch_force_t<SIM, PREC_MIXED, false>(c);
+    return meas ? launch_force_t<SIM, PREC_FP64, true>(c) : launch_force_t<SIM, PREC_FP64, false>(c);
+}
+
+static int enqueue_force_body(yk_ctx* c, bool meas)
+{
+    switch (c->p.sim_type) {
+    case YK_SIM_PURE_ION: return launch_force_s<SIM_PURE>(c, meas);
+    case YK_SIM_ION_MIXTURE: return launch_force_s<SIM_MIX>(c, meas);
+    case YK_SIM_NUCLEON: return launch_force_s<SIM_NUCLEON>(c, meas);
+    default:  // 'B-field': a = 0 (int_control.f:80-81)
+        cudaMemsetAsync(c->a, 0, sizeof(double) * 3 * (size_t)(c->n + 3), c->stream);
+        return 0;
+    }
+}
 
 // Returns the number of kernels enqueued.  Under yk_perf_enable the force
-// kernel is bracketed by an event pair (events are consumed in pairs).
+// call is bracketed by an event pair (events are consumed in pairs).
 static int enqueue_force(yk_ctx* c, bool meas, bool timed = false)
 {
     if (!timed) return enqueue_force_body(c, meas);
@@ -240,43 +397,40 @@ static int enqueue_force(yk_ctx* c, bool meas, bool timed = false)
     return k;
 }
 
-static int enqueue_force_body(yk_ctx* c, bool meas)
-{
-    switch (c->p.sim_type) {
-    case YK_SIM_PURE_ION: launch_force_s<SIM_PURE>(c, meas); return 1;
-    case YK_SIM_ION_MIXTURE: launch_force_s<SIM_MIX>(c, meas); return 1;
-    case YK_SIM_NUCLEON: launch_force_s<SIM_NUCLEON>(c, meas); return 1;
-    default:  // 'B-field': a = 0 (int_control.f:80-81)
-        cudaMemsetAsync(c->a, 0, sizeof(double) * 3 * (size_t)(c->n + 3), c->stream);
-        return 0;
-    }
-}
-
 static int enqueue_finish(yk_ctx* c, bool meas, int kin_mode, bool series)
 {
     FinishArgs z = c->fz_base;
     const bool has_force = c->p.sim_type != YK_SIM_BFIELD;
     z.force_mode = has_force ? 1 : 0;
-    z.nfp = (has_force && meas) ? c->nfb : 0;
     z.do_meas = meas ? 1 : 0;
+    if (c->kernel == 2) {
+        z.nfp = (has_force && meas) ? c->pj.njobs : 0;
+        z.half = 1.0;                   // each unique pair counted once
+    } else {
+        z.nfp = (has_force && meas) ? c->nfb : 0;
+        z.half = 0.5;                   // each pair counted from both sides
+    }
     z.kin_mode = kin_mode;
     z.nkp = (kin_mode == 2) ? c->nvb : 0;
-    k_finish<<<1, 256, 0, c->stream>>>(c->fpart, c->kpart, z, c->a, c->ds,
+    k_finish<<<1, 256, 0, c->stream>>>(c->kernel == 2 ? c->Sm : c->fpart, c->kpart, z, c->a, c->ds,
                                        series ? c->series : nullptr, c->series_idx);
     return 1;
 }
 
-// One integrator step; returns kernels enqueued.
-static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool timed = false)
+// One integrator step; returns kernels enqueued.  resort: refresh the
+// Morton order before the step.
+static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool resort, bool timed = false)
 {
     int k = 0;
+    if (resort || c->need_sort) k += enqueue_order(c, true);
+    else if (c->pos_dirty) k += enqueue_order(c, false);
     const int nb = c->nvb;
     cudaStream_t st = c->stream;
     const StepArgs& s = c->sa;
     switch (c->p.integrator) {
-    case YK_VV1: k_drift_vv1<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->pos, s); break;
-    case YK_VV3: k_drift_vv3<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->aii, c->pos, s); break;
-    default: k_drift_vv2<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->vold, c->a, c->zii, c->pos, s); break;
+    case YK_VV1: k_drift_vv1<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->iperm, c->pos, s); break;
+    case YK_VV3: k_drift_vv3<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->aii, c->iperm, c->pos, s); break;
+    default: k_drift_vv2<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->vold, c->a, c->zii, c->iperm, c->pos, s); break;
     }
     ++k;
     k += enqueue_force(c, meas, timed);
@@ -307,12 +461,9 @@ static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool timed = false)
     return k;
 }
 
-static int enqueue_pack(yk_ctx* c)
+static bool sort_due(const yk_ctx* c, long long step)
 {
-    if (!c->pos_dirty) return 0;
-    k_pack<<<c->nvb, VBLOCK, 0, c->stream>>>(c->x, c->zii, c->pos, c->n, c->sa.pack_w);
-    c->pos_dirty = false;
-    return 1;
+    return c->sort_every > 0 && step % c->sort_every == 0;
 }
 
 // Copy scalars and the error word back and wait for the stream.
@@ -372,6 +523,78 @@ static int check_params(const yk_params* p)
     return YK_OK;
 }
 
+static int finish_run(yk_ctx* c, int nsteps, bool want_series, yk_scalars* series)
+{
+    if (want_series) {
+        std::vector<double> h(13 * (size_t)nsteps);
+        CK(c, cudaMemcpy(h.data(), c->series, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < nsteps; ++s) {
+            const double* o = &h[13 * (size_t)s];
+            c->time = c->time + c->p.dt;
+            series[s].ev = o[0];
+            series[s].vir = o[1];
+            series[s].px = o[2];
+            series[s].ek = o[3];
+            for (int q = 0; q < 9; ++q) series[s].pp[q] = o[4 + q];
+            series[s].time = c->time;
+        }
+    } else {
+        for (int s = 0; s < nsteps; ++s) c->time = c->time + c->p.dt;
+    }
+    return YK_OK;
+}
+
+// Graph of K steps starting at a step count divisible by sort_every (so the
+// sort falls on local step 0) with measuring phase `phase` (local step l,
+// 1-based, measures when (phase + l) % me == 0).
+static GraphEntry* get_graph(yk_ctx* c, int K, int me, int phase, bool series, int* rc)
+{
+    *rc = YK_OK;
+    for (auto& g : c->graphs)
+        if (g.K == K && g.me == me && g.phase == phase && g.series == (series ? 1 : 0)) {
+            g.stamp = ++c->graph_clock;
+            return &g;
+        }
+    if ((int)c->graphs.size() >= MAX_GRAPHS) {
+        auto it = std::min_element(c->graphs.begin(), c->graphs.end(),
+                                   [](const GraphEntry& u, const GraphEntry& w) { return u.stamp < w.stamp; });
+        cudaGraphExecDestroy(it->exec);
+        c->graphs.erase(it);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        *rc = fail(c, YK_ERR_CUDA, "graph capture begin: %s", cudaGetErrorString(e));
+        return nullptr;
+    }
+    int kernels = 0;
+    for (int l = 1; l <= K; ++l) {
+        const bool meas = me > 0 && (phase + l) % me == 0;
+        const bool resort = c->sort_every > 0 && (l - 1) % c->sort_every == 0;
+        kernels += enqueue_newton(c, meas, series, resort);
+    }
+    e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) {
+        *rc = fail(c, YK_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+        return nullptr;
+    }
+    GraphEntry ent;
+    e = cudaGraphInstantiate(&ent.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        *rc = fail(c, YK_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+        return nullptr;
+    }
+    ent.K = K;
+    ent.me = me;
+    ent.phase = phase;
+    ent.series = series ? 1 : 0;
+    ent.kernels = kernels;
+    ent.stamp = ++c->graph_clock;
+    c->graphs.push_back(ent);
+    return &c->graphs.back();
+}
+
 // ---------------------------------------------------------------------------
 // C-ABI
 
@@ -409,26 +632,17 @@ const char* yk_last_error(const yk_ctx* ctx)
 
 int yk_destroy(yk_ctx* c)
 {
-    if (!c) return YK_ERR_ARG;
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    drop_graph(c);
-    cudaFree(c->x);
-    cudaFree(c->v);
-    cudaFree(c->vold);
-    cudaFree(c->a);
-    cudaFree(c->zii);
-    cudaFree(c->aii);
-    cudaFree(c->pos);
-    cudaFree(c->fpart);
-    cudaFree(c->kpart);
-    cudaFree(c->ds);
-    cudaFree(c->err);
-    cudaFree(c->series);
-    cudaFree(c->series_idx);
+    drop_graphs(c);
+    free_pairs(c);
+    void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->perm, c->iperm,
+                    c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->ds, c->err,
+                    c->series, c->series_idx, c->job_counter, c->flush_buf};
+    for (void* b : bufs) cudaFree(b);
     cudaFreeHost(c->h_ds);
     cudaFreeHost(c->h_err);
-    cudaFree(c->flush_buf);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -474,9 +688,14 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     setup_args(c);
 
     // HBM admission: refuse up front rather than fail half-way.
-    const size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
-                         sizeof(double4) * (size_t)n +
-                         sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;
+    size_t cub_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned*)nullptr, (unsigned*)nullptr,
+                                    (int*)nullptr, (int*)nullptr, n, 0, 30);
+    size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
+                   sizeof(double4) * (size_t)n + sizeof(int) * 5 * (size_t)n + cub_bytes +
+                   sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;
+    const bool pairs_fit = pair_scratch_bytes(n, c->seg) <= PAIR_SCRATCH_BUDGET;
+    if (pairs_fit) bytes += pair_scratch_bytes(n, c->seg);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         delete c;
@@ -501,12 +720,23 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     ALLOC(c->zii, n);
     ALLOC(c->aii, n);
     ALLOC(c->pos, n);
+    ALLOC(c->perm, n);
+    ALLOC(c->iperm, n);
+    ALLOC(c->keys0, n);
+    ALLOC(c->keys1, n);
+    ALLOC(c->idx0, n);
     ALLOC(c->fpart, 8 * (size_t)c->nfb);
     ALLOC(c->kpart, NKIN * (size_t)c->nvb);
     ALLOC(c->ds, 1);
     ALLOC(c->err, 1);
     ALLOC(c->series_idx, 1);
+    ALLOC(c->job_counter, 1);
 #undef ALLOC
+    c->cub_bytes = cub_bytes;
+    if (cudaMalloc(&c->cub_tmp, std::max<size_t>(cub_bytes, 16)) != cudaSuccess) {
+        yk_destroy(c);
+        return fail(nullptr, YK_ERR_NOMEM, "sort scratch");
+    }
     if (cudaMallocHost((void**)&c->h_ds, sizeof(DevScalars)) != cudaSuccess ||
         cudaMallocHost((void**)&c->h_err, sizeof(unsigned)) != cudaSuccess) {
         yk_destroy(c);
@@ -515,6 +745,11 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         yk_destroy(c);
         return fail(nullptr, YK_ERR_CUDA, "stream creation failed");
+    }
+    if ((rc = resolve_kernel(c)) != YK_OK) {
+        std::string m = c->errmsg;
+        yk_destroy(c);
+        return fail(nullptr, rc, "%s", m.c_str());
     }
     cudaStream_t st = c->stream;
     std::vector<double> fill(n);
@@ -539,8 +774,8 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     cudaMemsetAsync(c->ds, 0, sizeof(DevScalars), st);
     cudaMemsetAsync(c->err, 0, sizeof(unsigned), st);
     cudaMemsetAsync(c->series_idx, 0, sizeof(int), st);
-    c->pos_dirty = true;
-    g_launches += enqueue_pack(c);
+    c->need_sort = true;
+    g_launches += enqueue_order(c, true);
     if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         yk_destroy(c);
         return fail(nullptr, YK_ERR_CUDA, "initial upload failed");
@@ -549,12 +784,43 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     return YK_OK;
 }
 
+int yk_get_tuning(yk_ctx* c, yk_tuning* out)
+{
+    if (!c || !out) return fail(c, YK_ERR_ARG, "ctx and out are required");
+    out->force_kernel = c->kernel_req == 0 ? 0 : c->kernel;
+    out->pair_seg = c->seg;
+    out->sort_every = c->sort_every;
+    out->graph_steps = c->graph_steps;
+    return YK_OK;
+}
+
+int yk_set_tuning(yk_ctx* c, const yk_tuning* t)
+{
+    if (!c || !t) return fail(c, YK_ERR_ARG, "ctx and tuning are required");
+    if (t->force_kernel < 0 || t->force_kernel > 2) return fail(c, YK_ERR_ARG, "force_kernel must be 0..2");
+    if (t->pair_seg < 0 || t->graph_steps < 0 || t->sort_every < -1)
+        return fail(c, YK_ERR_ARG, "bad tuning values");
+    CK(c, cudaSetDevice(c->dev));
+    CK(c, cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->kernel_req = t->force_kernel;
+    c->seg = t->pair_seg > 0 ? t->pair_seg : DEFAULT_SEG;
+    const int old_sort = c->sort_every;
+    c->sort_every = t->sort_every == 0 ? DEFAULT_SORT_EVERY : t->sort_every;
+    c->graph_steps = t->graph_steps > 0 ? t->graph_steps : DEFAULT_GRAPH_STEPS;
+    if (old_sort != c->sort_every) c->need_sort = true;
+    int rc = resolve_kernel(c);
+    if (rc) return rc;
+    return YK_OK;
+}
+
 int yk_accel(yk_ctx* c, int do_meas, double* a_out, yk_scalars* out)
 {
     if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
     CK(c, cudaSetDevice(c->dev));
     const bool meas = do_meas != 0;
-    int k = enqueue_pack(c);
+    int k = 0;
+    if (c->need_sort || c->pos_dirty) k += enqueue_order(c, c->need_sort);
     k += enqueue_force(c, meas);
     k += enqueue_finish(c, meas, 0, false);
     g_launches += k;
@@ -571,37 +837,13 @@ int yk_newton(yk_ctx* c, int do_meas, yk_scalars* out)
 {
     if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
     CK(c, cudaSetDevice(c->dev));
-    int k = enqueue_pack(c);
-    k += enqueue_newton(c, do_meas != 0, false);
+    int k = enqueue_newton(c, do_meas != 0, false, sort_due(c, c->step_count));
     g_launches += k;
     int rc = sync_and_check(c);
     if (rc) return rc;
+    c->step_count += 1;
     c->time = c->time + c->p.dt;            // vel_verlet_2.f:114
     fill_scalars(c, out);
-    return YK_OK;
-}
-
-static int finish_run(yk_ctx* c, int nsteps, bool want_series, yk_scalars* series);
-
-static int capture_graph(yk_ctx* c, int K, int me, bool series)
-{
-    drop_graph(c);
-    cudaGraph_t g = nullptr;
-    CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int kernels = 0;
-    for (int s = 1; s <= K; ++s) kernels += enqueue_newton(c, me > 0 && s % me == 0, series);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    if (e != cudaSuccess) return fail(c, YK_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&c->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-        c->graph = nullptr;
-        return fail(c, YK_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-    }
-    c->graph_K = K;
-    c->graph_me = me;
-    c->graph_series = series ? 1 : 0;
-    c->graph_kernels = kernels;
     return YK_OK;
 }
 
@@ -613,7 +855,7 @@ int yk_run(yk_ctx* c, int nsteps, int meas_every, yk_scalars* series)
     CK(c, cudaSetDevice(c->dev));
     const bool want_series = series != nullptr;
     if (want_series && c->series_cap < nsteps) {
-        drop_graph(c);
+        drop_graphs(c);
         cudaFree(c->series);
         c->series = nullptr;
         c->series_cap = 0;
@@ -621,16 +863,19 @@ int yk_run(yk_ctx* c, int nsteps, int meas_every, yk_scalars* series)
         c->series_cap = nsteps;
     }
     CK(c, cudaMemsetAsync(c->series_idx, 0, sizeof(int), c->stream));
-    int k = enqueue_pack(c);
+    const int me = meas_every;
+    auto meas_at = [&](int s) { return me > 0 && s % me == 0; };
+    int k = 0;
     if (c->perf_on) {
-        // Timed path: step by step, event pairs around every force kernel.
+        // Timed path: step by step, event pairs around every force call.
         c->ev_used = 0;
         cudaEvent_t e0 = next_event(c), e1 = next_event(c);
         CK(c, cudaEventRecord(e0, c->stream));
         for (int s = 1; s <= nsteps; ++s) {
             if (c->flush_bytes)
                 CK(c, cudaMemsetAsync(c->flush_buf, s & 0xff, c->flush_bytes, c->stream));
-            k += enqueue_newton(c, meas_every > 0 && s % meas_every == 0, want_series, true);
+            k += enqueue_newton(c, meas_at(s), want_series, sort_due(c, c->step_count), true);
+            c->step_count += 1;
         }
         CK(c, cudaEventRecord(e1, c->stream));
         g_launches += k;
@@ -647,51 +892,35 @@ int yk_run(yk_ctx* c, int nsteps, int meas_every, yk_scalars* series)
         c->perf.steps += nsteps;
         return finish_run(c, nsteps, want_series, series);
     }
-    // K steps per graph: a multiple of meas_every near 50 so that every
-    // launch of the graph has the same measuring pattern.
-    int K = 50;
-    if (meas_every > 0) K = meas_every * ((50 + meas_every - 1) / meas_every);
-    if (K > nsteps) K = 0;
-    int done = 0;
-    if (K > 0) {
-        if (!(c->graph && c->graph_K == K && c->graph_me == meas_every &&
-              c->graph_series == (want_series ? 1 : 0))) {
-            int rc = capture_graph(c, K, meas_every, want_series);
-            if (rc) return rc;
-        }
-        while (done + K <= nsteps) {
-            CK(c, cudaGraphLaunch(c->graph, c->stream));
-            k += c->graph_kernels;
-            done += K;
-        }
+    // Eager steps until the step count is aligned with the sort cadence,
+    // then graphs of K steps (K a multiple of sort_every), then the rest.
+    int s = 1;
+    const int K = c->sort_every > 0
+                      ? c->sort_every * std::max(1, c->graph_steps / c->sort_every)
+                      : c->graph_steps;
+    while (s <= nsteps && c->sort_every > 0 && c->step_count % c->sort_every != 0) {
+        k += enqueue_newton(c, meas_at(s), want_series, sort_due(c, c->step_count));
+        c->step_count += 1;
+        ++s;
     }
-    for (int s = done + 1; s <= nsteps; ++s)
-        k += enqueue_newton(c, meas_every > 0 && s % meas_every == 0, want_series);
+    if (c->pos_dirty || c->need_sort) k += enqueue_order(c, c->need_sort);
+    while (s + K - 1 <= nsteps) {
+        int rc = YK_OK;
+        GraphEntry* g = get_graph(c, K, me, me > 0 ? (s - 1) % me : 0, want_series, &rc);
+        if (!g) return rc;
+        CK(c, cudaGraphLaunch(g->exec, c->stream));
+        k += g->kernels;
+        c->step_count += K;
+        s += K;
+    }
+    for (; s <= nsteps; ++s) {
+        k += enqueue_newton(c, meas_at(s), want_series, sort_due(c, c->step_count));
+        c->step_count += 1;
+    }
     g_launches += k;
     int rc = sync_and_check(c);
     if (rc) return rc;
     return finish_run(c, nsteps, want_series, series);
-}
-
-static int finish_run(yk_ctx* c, int nsteps, bool want_series, yk_scalars* series)
-{
-    if (want_series) {
-        std::vector<double> h(13 * (size_t)nsteps);
-        CK(c, cudaMemcpy(h.data(), c->series, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
-        for (int s = 0; s < nsteps; ++s) {
-            const double* o = &h[13 * (size_t)s];
-            c->time = c->time + c->p.dt;
-            series[s].ev = o[0];
-            series[s].vir = o[1];
-            series[s].px = o[2];
-            series[s].ek = o[3];
-            for (int q = 0; q < 9; ++q) series[s].pp[q] = o[4 + q];
-            series[s].time = c->time;
-        }
-    } else {
-        for (int s = 0; s < nsteps; ++s) c->time = c->time + c->p.dt;
-    }
-    return YK_OK;
 }
 
 int yk_get_state(yk_ctx* c, double* x, double* v, double* vold, double* a)
@@ -721,8 +950,9 @@ int yk_set_state(yk_ctx* c, const double* x, const double* v, const double* vold
     if (vold) CK(c, cudaMemcpyAsync(c->vold, vold, b, cudaMemcpyHostToDevice, c->stream));
     if (a) CK(c, cudaMemcpyAsync(c->a, a, b, cudaMemcpyHostToDevice, c->stream));
     if (x) {
+        // keep the current Morton order; the next scheduled sort refreshes it
         c->pos_dirty = true;
-        g_launches += enqueue_pack(c);
+        g_launches += enqueue_order(c, false);
     }
     CK(c, cudaStreamSynchronize(c->stream));
     return YK_OK;
@@ -733,9 +963,12 @@ int yk_set_box(yk_ctx* c, const double xl[3])
     if (!c || !xl) return fail(c, YK_ERR_ARG, "ctx and xl are required");
     for (int k = 0; k < 3; ++k)
         if (!(xl[k] > 0.0) || !std::isfinite(xl[k])) return fail(c, YK_ERR_ARG, "xl must be > 0");
+    bool same = true;
+    for (int k = 0; k < 3; ++k) same = same && c->p.xl[k] == xl[k];
+    if (same) return YK_OK;
     for (int k = 0; k < 3; ++k) c->p.xl[k] = xl[k];
     setup_args(c);
-    drop_graph(c);
+    drop_graphs(c);
     return YK_OK;
 }
 
@@ -801,7 +1034,7 @@ int yk_peak_probe(int device, int kind, double* tflops)
 
 int yk_host_register(void* ptr, size_t bytes)
 {
-    if (!ptr || !bytes) return YK_ERR_ARG;
+    if (!ptr || !bytes) return fail(nullptr, YK_ERR_ARG, "bad host buffer");
     cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
     if (e != cudaSuccess) return fail(nullptr, YK_ERR_CUDA, "cudaHostRegister: %s", cudaGetErrorString(e));
     return YK_OK;
@@ -809,7 +1042,7 @@ int yk_host_register(void* ptr, size_t bytes)
 
 int yk_host_unregister(void* ptr)
 {
-    if (!ptr) return YK_ERR_ARG;
+    if (!ptr) return fail(nullptr, YK_ERR_ARG, "bad host buffer");
     cudaError_t e = cudaHostUnregister(ptr);
     if (e != cudaSuccess) return fail(nullptr, YK_ERR_CUDA, "cudaHostUnregister: %s", cudaGetErrorString(e));
     return YK_OK;

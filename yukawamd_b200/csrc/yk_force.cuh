@@ -1,31 +1,33 @@
-// yk_force.cuh -- O(N^2) minimum-image pair-force kernels.
+// yk_force.cuh -- pair physics and the "row" force kernel.
 //
 // Reference routines (one pass over all pairs per force call):
 //   accel_ion_pure  int_ion_pure.f:98-254   screened Coulomb, one species
 //   accel_ion_mix   int_ion_mix.f:105-295   screened Coulomb, Z_i Z_j weights
 //   accel_nn        int_nn.f:130-345        HPP Gaussians + p-p screened Coulomb
 //
-// Kernel k_force_rows ("row" form): every thread owns one target particle i
-// and keeps its position and its force / energy / virial / pressure-tensor
-// sums in registers; the CTA streams the whole source array through shared
-// memory in tiles of FTILE particles, each tile a single 1-D TMA bulk copy
-// (double-buffered on two mbarriers).  Each pair is evaluated from both
-// sides (N(N-1) evaluations), so no thread ever writes another particle's
-// force: forces need no atomics and no scratch, and every per-particle sum
-// runs in the fixed order j = 0..n-1.  The scalar sums (U, virial, P) are
-// reduced per CTA into a partials array and finished by k_finalize.
-//
-// Physics per pair (d = x_i - x_j after minimum image, r = |d|):
-//   ion:  u = e^{-mu r}/r - evcut,  f = (1 + mu r) e^{-mu r}/r^3   (x Z_j for
-//         the mixture), F_i += f d, W += f r^2, P += d (f d)
+// Physics per pair (d = x_i - x_j after minimum image, r = |d|); the pair
+// functions return the scalar fs with F_i += fs d, plus u and w = fs r^2 for
+// measurements:
+//   ion:  u = e^{-mu r}/r - evcut,  fs = (1 + mu r) e^{-mu r}/r^3
+//         (the mixture's Z_j / Z_i weights are applied by the caller, exactly
+//         where int_ion_mix.f:179-180 applies them)
 //   nn:   nuclear (r^2 <= rncut^2): e = exp(-r^2/(2 Lambda)),
-//         u = (aa e + B) e, f = (2 aa e + B) e / Lambda, B = bb +/- cc by
+//         u = (aa e + B) e, fs = (2 aa e + B) e / Lambda, B = bb +/- cc by
 //         species equality; Coulomb (p-p, r^2 <= rccut^2): vc x the ion terms.
 //
-// PREC_FP64: all FP64 (exp(), rsqrt() from the CUDA math library).
-// PREC_MIXED: displacement and minimum image in FP64, then cast to FP32;
-// the r^2, rsqrt, exp and force terms in FP32; per-particle force sums in
-// compensated FP32 (two-sum), folded to FP64 in the epilogue.
+// PREC_FP64: all FP64 (exp(), rsqrt() from the CUDA math library; rsqrt
+// replaces the reference's sqrt and divide, 1/(r r^2) = rinv^3).
+// PREC_MIXED: displacement and minimum image in FP64, then cast to FP32; the
+// r^2, rsqrt, exp and force terms in FP32.
+//
+// Particles are addressed by "slot": the engine keeps them in a Morton
+// (space-filling-curve) order so that the 32 targets of a warp are close in
+// space and mostly leave or enter the cutoff sphere together.  perm[slot] is
+// the caller's particle index; outputs are scattered back through it.
+//
+// Kernel k_force_rows: every thread owns one target slot and sums over all
+// N-1 sources (each pair evaluated from both sides, no scratch).  The
+// default engine kernel is k_force_pairs in yk_pairs.cuh.
 #pragma once
 
 #include <type_traits>
@@ -36,7 +38,7 @@ namespace yk {
 
 constexpr int SIM_NUCLEON = 1, SIM_PURE = 2, SIM_MIX = 3;
 constexpr int PREC_FP64 = 0, PREC_MIXED = 1;
-constexpr int FBLOCK = 128;          // threads per CTA = target particles per CTA
+constexpr int FBLOCK = 128;          // threads per CTA of the row kernel
 constexpr int FTILE = 128;           // source particles per shared-memory tile
 constexpr int NSCAL = 8;             // U, W, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz
 
@@ -53,168 +55,106 @@ struct ForceArgs {
     int n, nuclear_on, coulomb_on, mix_compat;
 };
 
-// ---- FP64 accumulators -------------------------------------------------
-template <bool MEAS>
-struct Acc64 {
-    double f[3];
-    double s[NSCAL];
-    __device__ __forceinline__ Acc64()
-    {
-        f[0] = f[1] = f[2] = 0.0;
-#pragma unroll
-        for (int k = 0; k < NSCAL; ++k) s[k] = 0.0;
-    }
-    __device__ __forceinline__ void add(double fs, double dx, double dy, double dz,
-                                        double u, double w)
-    {
-        const double fx = fs * dx, fy = fs * dy, fz = fs * dz;
-        f[0] += fx;
-        f[1] += fy;
-        f[2] += fz;
-        if constexpr (MEAS) {
-            s[0] += u;
-            s[1] += w;
-            s[2] += dx * fx;
-            s[3] += dx * fy;
-            s[4] += dx * fz;
-            s[5] += dy * fy;
-            s[6] += dy * fz;
-            s[7] += dz * fz;
-        }
-    }
+template <typename R>
+struct PairOut {
+    R fs, u, w;
+    R dx, dy, dz;
+    bool hit;
 };
 
-// ---- compensated FP32 accumulators --------------------------------------
-template <bool MEAS>
-struct AccMixed {
-    cf32 f[3];
-    cf32 s[MEAS ? NSCAL : 1];
-    __device__ __forceinline__ void add(float fs, float dx, float dy, float dz, float u, float w)
-    {
-        const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
-        f[0].add(fx);
-        f[1].add(fy);
-        f[2].add(fz);
-        if constexpr (MEAS) {
-            s[0].add(u);
-            s[1].add(w);
-            s[2].add(dx * fx);
-            s[3].add(dx * fy);
-            s[4].add(dx * fz);
-            s[5].add(dy * fy);
-            s[6].add(dy * fz);
-            s[7].add(dz * fz);
-        }
-    }
-};
-
-// ---- one directed pair, FP64 --------------------------------------------
+// ---- one pair, FP64 -------------------------------------------------------
 template <int SIM, bool MEAS>
-__device__ __forceinline__ void pair_eval(const ForceArgs& fa, const double4& pi, const double4& pj,
-                                          bool distinct, Acc64<MEAS>& acc)
+__device__ __forceinline__ void pair64(const ForceArgs& fa, const double4& pi, const double4& pj,
+                                       bool valid, PairOut<double>& o)
 {
-    const double dx = min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]);
-    const double dy = min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]);
-    const double dz = min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]);
-    const double r2 = dx * dx + dy * dy + dz * dz;
+    o.dx = min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]);
+    o.dy = min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]);
+    o.dz = min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]);
+    const double r2 = o.dx * o.dx + o.dy * o.dy + o.dz * o.dz;
+    o.fs = 0.0;
+    o.u = 0.0;
+    o.w = 0.0;
+    o.hit = false;
     if constexpr (SIM == SIM_PURE || SIM == SIM_MIX) {
-        if (distinct && r2 <= fa.rc2) {
+        if (valid && r2 <= fa.rc2) {
             const double rinv = rsqrt(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;
-            const double er = exp(-mr) * rinv;               // e^{-mu r}/r
-            double fs = (1.0 + mr) * er * (rinv * rinv);      // (1+mu r) e^{-mu r}/r^3
-            double u = 0.0, w = 0.0;
-            if (MEAS) {
-                u = er - fa.evcut;
-                w = fs * r2;
+            const double er = exp(-mr) * rinv;                // e^{-mu r}/r
+            o.fs = (1.0 + mr) * er * (rinv * rinv);           // (1+mu r) e^{-mu r}/r^3
+            if constexpr (MEAS) {
+                o.u = er - fa.evcut;
+                o.w = o.fs * r2;
             }
-            if constexpr (SIM == SIM_MIX) {
-                fs *= pj.w;
-                if constexpr (MEAS) {
-                    u *= pj.w;
-                    w *= pj.w;
-                }
-            }
-            acc.add(fs, dx, dy, dz, u, w);
+            o.hit = true;
         }
     } else {
-        if (!distinct) return;
-        double fs = 0.0, u = 0.0, w = 0.0;
-        bool hit = false;
+        if (!valid) return;
         if (fa.nuclear_on && r2 <= fa.rn2) {
             const double e = exp(-(r2 * fa.xp2i));
             const double B = (pi.w == pj.w) ? fa.bpc : fa.bmc;
             const double fn = fa.xpi * (fa.aa2 * e + B) * e;
-            fs = fn;
-            if (MEAS) {
-                u = (fa.aa * e + B) * e;
-                w = fn * r2;
+            o.fs = fn;
+            if constexpr (MEAS) {
+                o.u = (fa.aa * e + B) * e;
+                o.w = fn * r2;
             }
-            hit = true;
+            o.hit = true;
         }
         if (fa.coulomb_on && pi.w == 1.0 && pj.w == 1.0 && r2 <= fa.rc2) {
             const double rinv = rsqrt(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;
-            const double er = fa.vc * exp(-mr) * rinv;        // vc e^{-mu r}/r
+            const double er = fa.vc * exp(-mr) * rinv;         // vc e^{-mu r}/r
             const double fc = (1.0 + mr) * er * (rinv * rinv);
-            fs += fc;
-            if (MEAS) {
-                u += er - fa.evcut;
-                w += fc * r2;
+            o.fs += fc;
+            if constexpr (MEAS) {
+                o.u += er - fa.evcut;
+                o.w += fc * r2;
             }
-            hit = true;
+            o.hit = true;
         }
-        if (hit) acc.add(fs, dx, dy, dz, u, w);
     }
 }
 
-// ---- one directed pair, mixed ------------------------------------------
+// ---- one pair, mixed ---------------------------------------------------------
 template <int SIM, bool MEAS>
-__device__ __forceinline__ void pair_eval(const ForceArgs& fa, const double4& pi, const double4& pj,
-                                           bool distinct, AccMixed<MEAS>& acc)
+__device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, const double4& pj,
+                                       bool valid, PairOut<float>& o)
 {
-    const float dx = __double2float_rn(min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]));
-    const float dy = __double2float_rn(min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]));
-    const float dz = __double2float_rn(min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]));
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    o.dx = __double2float_rn(min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]));
+    o.dy = __double2float_rn(min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]));
+    o.dz = __double2float_rn(min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]));
+    const float r2 = fmaf(o.dx, o.dx, fmaf(o.dy, o.dy, o.dz * o.dz));
+    o.fs = 0.f;
+    o.u = 0.f;
+    o.w = 0.f;
+    o.hit = false;
     if constexpr (SIM == SIM_PURE || SIM == SIM_MIX) {
-        if (distinct && r2 <= fa.rc2f) {
+        if (valid && r2 <= fa.rc2f) {
             const float rinv = rsqrt_f32(r2);
             const float r = r2 * rinv;
             const float mr = fa.xmucf * r;
             const float er = exp_neg_f32(mr) * rinv;
-            float fs = (1.0f + mr) * er * (rinv * rinv);
-            float u = 0.f, w = 0.f;
-            if (MEAS) {
-                u = er - fa.evcutf;
-                w = fs * r2;
+            o.fs = (1.0f + mr) * er * (rinv * rinv);
+            if constexpr (MEAS) {
+                o.u = er - fa.evcutf;
+                o.w = o.fs * r2;
             }
-            if constexpr (SIM == SIM_MIX) {
-                const float zj = (float)pj.w;
-                fs *= zj;
-                if constexpr (MEAS) {
-                    u *= zj;
-                    w *= zj;
-                }
-            }
-            acc.add(fs, dx, dy, dz, u, w);
+            o.hit = true;
         }
     } else {
-        if (!distinct) return;
-        float fs = 0.f, u = 0.f, w = 0.f;
-        bool hit = false;
+        if (!valid) return;
         if (fa.nuclear_on && r2 <= fa.rn2f) {
             const float e = exp_neg_f32(r2 * fa.xp2if);
             const float B = (pi.w == pj.w) ? fa.bpcf : fa.bmcf;
             const float fn = fa.xpif * fmaf(fa.aa2f, e, B) * e;
-            fs = fn;
-            if (MEAS) {
-                u = fmaf(fa.aaf, e, B) * e;
-                w = fn * r2;
+            o.fs = fn;
+            if constexpr (MEAS) {
+                o.u = fmaf(fa.aaf, e, B) * e;
+                o.w = fn * r2;
             }
-            hit = true;
+            o.hit = true;
         }
         if (fa.coulomb_on && pi.w == 1.0 && pj.w == 1.0 && r2 <= fa.rc2f) {
             const float rinv = rsqrt_f32(r2);
@@ -222,55 +162,143 @@ __device__ __forceinline__ void pair_eval(const ForceArgs& fa, const double4& pi
             const float mr = fa.xmucf * r;
             const float er = fa.vcf * exp_neg_f32(mr) * rinv;
             const float fc = (1.0f + mr) * er * (rinv * rinv);
-            fs += fc;
-            if (MEAS) {
-                u += er - fa.evcutf;
-                w += fc * r2;
+            o.fs += fc;
+            if constexpr (MEAS) {
+                o.u += er - fa.evcutf;
+                o.w += fc * r2;
             }
-            hit = true;
+            o.hit = true;
         }
-        if (hit) acc.add(fs, dx, dy, dz, u, w);
     }
 }
 
-// ---- epilogue: scale to accelerations (int_ion_pure.f:227-231,
-// int_ion_mix.f:273-277 with the fold of :201, int_nn.f:318-322) ----------
+// ---- per-target accumulators --------------------------------------------
+// FP64 form: plain double sums.  Mixed form: Knuth two-sum FP32 sums.
+template <int PREC, bool MEAS>
+struct TargetAcc;
+
+template <bool MEAS>
+struct TargetAcc<PREC_FP64, MEAS> {
+    double f[3];
+    double s[MEAS ? NSCAL : 1];
+    __device__ __forceinline__ void zero()
+    {
+        f[0] = f[1] = f[2] = 0.0;
+#pragma unroll
+        for (int k = 0; k < (MEAS ? NSCAL : 1); ++k) s[k] = 0.0;
+    }
+    // weight: Z_j for the mixture (int_ion_mix.f:179), 1 otherwise
+    __device__ __forceinline__ void add(const PairOut<double>& o, double weight)
+    {
+        const double fs = o.fs * weight;
+        const double fx = fs * o.dx, fy = fs * o.dy, fz = fs * o.dz;
+        f[0] += fx;
+        f[1] += fy;
+        f[2] += fz;
+        if constexpr (MEAS) {
+            s[0] += o.u * weight;
+            s[1] += o.w * weight;
+            s[2] += o.dx * fx;
+            s[3] += o.dx * fy;
+            s[4] += o.dx * fz;
+            s[5] += o.dy * fy;
+            s[6] += o.dy * fz;
+            s[7] += o.dz * fz;
+        }
+    }
+    __device__ __forceinline__ double force(int k) const { return f[k]; }
+    __device__ __forceinline__ double scal(int k) const
+    {
+        if constexpr (MEAS) return s[k];
+        return 0.0;
+    }
+};
+
+template <bool MEAS>
+struct TargetAcc<PREC_MIXED, MEAS> {
+    cf32 f[3];
+    cf32 s[MEAS ? NSCAL : 1];
+    __device__ __forceinline__ void zero()
+    {
+        f[0] = f[1] = f[2] = cf32();
+#pragma unroll
+        for (int k = 0; k < (MEAS ? NSCAL : 1); ++k) s[k] = cf32();
+    }
+    __device__ __forceinline__ void add(const PairOut<float>& o, float weight)
+    {
+        const float fs = o.fs * weight;
+        const float fx = fs * o.dx, fy = fs * o.dy, fz = fs * o.dz;
+        f[0].add(fx);
+        f[1].add(fy);
+        f[2].add(fz);
+        if constexpr (MEAS) {
+            s[0].add(o.u * weight);
+            s[1].add(o.w * weight);
+            s[2].add(o.dx * fx);
+            s[3].add(o.dx * fy);
+            s[4].add(o.dx * fz);
+            s[5].add(o.dy * fy);
+            s[6].add(o.dy * fz);
+            s[7].add(o.dz * fz);
+        }
+    }
+    __device__ __forceinline__ double force(int k) const { return f[k].value(); }
+    __device__ __forceinline__ double scal(int k) const
+    {
+        if constexpr (MEAS) return s[k].value();
+        return 0.0;
+    }
+};
+
+template <int PREC>
+using real_t = std::conditional_t<PREC == PREC_FP64, double, float>;
+
+template <int SIM, int PREC, bool MEAS>
+__device__ __forceinline__ void pair_eval(const ForceArgs& fa, const double4& pi, const double4& pj,
+                                          bool valid, PairOut<real_t<PREC>>& o)
+{
+    if constexpr (PREC == PREC_FP64) pair64<SIM, MEAS>(fa, pi, pj, valid, o);
+    else pair32<SIM, MEAS>(fa, pi, pj, valid, o);
+}
+
+// ---- scaling to accelerations (int_ion_pure.f:227-231, int_ion_mix.f:273-277
+// with the fold fj(:,i) = zii(i)*(fj(:,i)+fi(:)) of :201, int_nn.f:318-322).
+// F is the sum of Z_j-weighted terms (mixture) or plain terms.  orig is the
+// caller's particle index; the fold is skipped for orig = n-1 in compat mode
+// because the reference's i loop ends at n-2 (int_ion_mix.f:158).
 template <int SIM>
-__device__ __forceinline__ void store_accel(const ForceArgs& fa, int i, double wi, const double* aii,
-                                            double F[3], double* a_out)
+__device__ __forceinline__ void store_accel(const ForceArgs& fa, int orig, double zi,
+                                            const double* __restrict__ aii, const double F[3],
+                                            double* __restrict__ a_out)
 {
     if constexpr (SIM == SIM_PURE) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) a_out[3 * i + k] = fa.coef * F[k] / fa.ai_xmass;
+        for (int k = 0; k < 3; ++k) a_out[3 * orig + k] = fa.coef * F[k] / fa.ai_xmass;
     } else if constexpr (SIM == SIM_MIX) {
-        // Reference fold fj(:,i) = zii(i)*(...) runs only for i <= n-2.
-        const bool fold = !(fa.mix_compat && i == fa.n - 1);
-        const double am = aii[i] * fa.xmass;
+        const bool fold = !(fa.mix_compat && orig == fa.n - 1);
+        const double am = aii[orig] * fa.xmass;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const double f = fold ? wi * F[k] : F[k];
-            a_out[3 * i + k] = fa.coef * f / am;
-        }
+        for (int k = 0; k < 3; ++k) a_out[3 * orig + k] = fa.coef * (fold ? zi * F[k] : F[k]) / am;
     } else {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) a_out[3 * i + k] = F[k] / fa.xmass;
+        for (int k = 0; k < 3; ++k) a_out[3 * orig + k] = F[k] / fa.xmass;
     }
 }
 
-// Shared memory of k_force_rows: 2 stages of FTILE double4, 2 mbarriers,
-// and the block-reduction scratch.
+// Shared memory of k_force_rows: 2 stages of FTILE double4, 2 mbarriers and
+// the block-reduction scratch.
 constexpr int FORCE_SMEM = 2 * FTILE * (int)sizeof(double4) + 16 + 32 * NSCAL * (int)sizeof(double);
 
 template <int SIM, int PREC, bool MEAS>
 __global__ void __launch_bounds__(FBLOCK)
-k_force_rows(const double4* __restrict__ pos, const double* __restrict__ aii, ForceArgs fa,
-             double* __restrict__ a_out, double* __restrict__ part, unsigned* __restrict__ err)
+k_force_rows(const double4* __restrict__ pos, const int* __restrict__ perm,
+             const double* __restrict__ aii, ForceArgs fa, double* __restrict__ a_out,
+             double* __restrict__ part, unsigned* __restrict__ err)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     double4* tile = reinterpret_cast<double4*>(smem);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * FTILE * sizeof(double4));
     double* red = reinterpret_cast<double*>(smem + 2 * FTILE * sizeof(double4) + 16);
-    __shared__ int s_abort;
 
     const int n = fa.n;
     const int i = blockIdx.x * FBLOCK + threadIdx.x;
@@ -279,7 +307,6 @@ k_force_rows(const double4* __restrict__ pos, const double* __restrict__ aii, Fo
     const int ntiles = (n + FTILE - 1) / FTILE;
 
     if (threadIdx.x == 0) {
-        s_abort = 0;
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         fence_mbar_init();
@@ -298,8 +325,9 @@ k_force_rows(const double4* __restrict__ pos, const double* __restrict__ aii, Fo
         if (ntiles > 1) issue(1);
     }
 
-    using Acc = std::conditional_t<PREC == PREC_FP64, Acc64<MEAS>, AccMixed<MEAS>>;
-    Acc acc;
+    TargetAcc<PREC, MEAS> acc;
+    acc.zero();
+    PairOut<real_t<PREC>> o;
 
     for (int t = 0; t < ntiles; ++t) {
         const int st = t & 1;
@@ -316,40 +344,27 @@ k_force_rows(const double4* __restrict__ pos, const double* __restrict__ aii, Fo
         const double4* tl = tile + st * FTILE;
         if (active) {
 #pragma unroll 2
-            for (int jj = 0; jj < cnt; ++jj)
-                pair_eval<SIM, MEAS>(fa, pi, tl[jj], (j0 + jj) != i, acc);
+            for (int jj = 0; jj < cnt; ++jj) {
+                const double4 pj = tl[jj];
+                pair_eval<SIM, PREC, MEAS>(fa, pi, pj, (j0 + jj) != i, o);
+                if (o.hit) acc.add(o, SIM == SIM_MIX ? (real_t<PREC>)pj.w : (real_t<PREC>)1);
+            }
         }
         __syncthreads();                      // every thread is done with stage st
         if (threadIdx.x == 0 && t + 2 < ntiles) issue(t + 2);
     }
 
-    double F[3], S[NSCAL];
+    double S[NSCAL];
 #pragma unroll
-    for (int k = 0; k < NSCAL; ++k) S[k] = 0.0;
-    if constexpr (PREC == PREC_FP64) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) F[k] = acc.f[k];
-        if constexpr (MEAS) {
-#pragma unroll
-            for (int k = 0; k < NSCAL; ++k) S[k] = acc.s[k];
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) F[k] = acc.f[k].value();
-        if constexpr (MEAS) {
-#pragma unroll
-            for (int k = 0; k < NSCAL; ++k) S[k] = acc.s[k].value();
-        }
+    for (int k = 0; k < NSCAL; ++k) S[k] = (MEAS && active) ? acc.scal(k) : 0.0;
+    if (active) {
+        const double F[3] = {acc.force(0), acc.force(1), acc.force(2)};
+        store_accel<SIM>(fa, perm[i], pi.w, aii, F, a_out);
     }
-    if (active) store_accel<SIM>(fa, i, pi.w, aii, F, a_out);
     if constexpr (MEAS) {
         if constexpr (SIM == SIM_MIX) {
 #pragma unroll
             for (int k = 0; k < NSCAL; ++k) S[k] *= pi.w;    // ev += zii(i)*evx ...
-        }
-        if (!active) {
-#pragma unroll
-            for (int k = 0; k < NSCAL; ++k) S[k] = 0.0;
         }
         block_sum_store<NSCAL>(S, red, part + (size_t)blockIdx.x * NSCAL);
     }

@@ -12,7 +12,8 @@
 // contracted into an FMA: positions and velocities come out bit-identical to
 // the reference's arithmetic (which is compiled without FMA) given the same
 // accelerations.  The drift kernels also pack the FP64 positions with the
-// per-particle weight (zii) into the double4 array the force kernels stream.
+// per-particle weight (zii) into the Morton-ordered double4 array the force
+// kernels stream (slot iperm[i] for particle i).
 #pragma once
 
 #include "yk_common.cuh"
@@ -45,19 +46,10 @@ __device__ __forceinline__ double drift1(double x, double v, double a, const Ste
     return wrap_once(__dadd_rn(__dadd_rn(x, __dmul_rn(v, s.dt)), __dmul_rn(s.afac, a)), s.xl[k]);
 }
 
-// Pack positions (no step): used after yk_set_state / yk_create.
-__global__ void k_pack(const double* __restrict__ x, const double* __restrict__ zii,
-                       double4* __restrict__ pos, int n, int pack_w)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    pos[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], pack_w ? zii[i] : 0.0);
-}
-
 // VV2 first half: drift, vold = v, v += dt a.
 __global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold,
                             const double* __restrict__ a, const double* __restrict__ zii,
-                            double4* __restrict__ pos, StepArgs s)
+                            const int* __restrict__ iperm, double4* __restrict__ pos, StepArgs s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
@@ -71,13 +63,13 @@ __global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, doub
         vold[e] = vi;
         v[e] = __dadd_rn(vi, __dmul_rn(s.dt, ai));
     }
-    pos[i] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
+    pos[iperm[i]] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
 }
 
 // VV1 first half: drift, v += dt/2 a (vel_verlet_1.f:148-166).
 __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
                             const double* __restrict__ a, const double* __restrict__ zii,
-                            double4* __restrict__ pos, StepArgs s)
+                            const int* __restrict__ iperm, double4* __restrict__ pos, StepArgs s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
@@ -90,14 +82,15 @@ __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
         x[e] = xn[k];
         v[e] = __dadd_rn(v[e], __dmul_rn(s.halfdt, ai));
     }
-    pos[i] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
+    pos[iperm[i]] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
 }
 
 // VV3 first half: drift and the first Spreiter-Walter stage
 // (vel_verlet_3.f:255-262; v(2,i) reads the already updated v(1,i)).
 __global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ v,
                             const double* __restrict__ a, const double* __restrict__ zii,
-                            const double* __restrict__ aii, double4* __restrict__ pos, StepArgs s)
+                            const double* __restrict__ aii, const int* __restrict__ iperm,
+                            double4* __restrict__ pos, StepArgs s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
@@ -121,7 +114,7 @@ __global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ v,
     v[3 * i] = v1;
     v[3 * i + 1] = v2;
     v[3 * i + 2] = v3;
-    pos[i] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
+    pos[iperm[i]] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
 }
 
 template <bool KIN>

@@ -114,6 +114,21 @@ class Engine:
         for k in range(3):
             self.params.xl[k] = float(xl[k])
 
+    # -- engine tunables (force kernel, job size, sort cadence, graph length) -
+    def tuning(self):
+        t = abi.YkTuning()
+        check(self._lib.yk_get_tuning(self._ctx, C.byref(t)), self._ctx)
+        return t
+
+    def set_tuning(self, force_kernel=None, pair_seg=None, sort_every=None, graph_steps=None):
+        t = self.tuning()
+        for name, val in (("force_kernel", force_kernel), ("pair_seg", pair_seg),
+                          ("sort_every", sort_every), ("graph_steps", graph_steps)):
+            if val is not None:
+                setattr(t, name, int(val))
+        check(self._lib.yk_set_tuning(self._ctx, C.byref(t)), self._ctx)
+        return self.tuning()
+
     # -- timers (the reference's perf.f newton / accel timers) --------------
     def perf_enable(self, enable=True, flush_bytes=0):
         check(self._lib.yk_perf_enable(self._ctx, int(bool(enable)), int(flush_bytes)),
