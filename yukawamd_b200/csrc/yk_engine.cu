@@ -74,6 +74,7 @@ struct yk_ctx {
     double *zii = nullptr, *aii = nullptr;
     // Morton order
     double4* pos = nullptr;
+    float* posf = nullptr;           // FP32 shadow of pos, tiled SoA (shadow_index)
     int *perm = nullptr, *iperm = nullptr;
     unsigned *keys0 = nullptr, *keys1 = nullptr;
     int* idx0 = nullptr;
@@ -193,6 +194,25 @@ static void setup_args(yk_ctx* c)
     f.aa2f = (float)f.aa2;
     f.bpcf = (float)f.bpc;
     f.bmcf = (float)f.bmc;
+    // FP32 screen: widen each radius by 2^-19 L (16 ulp of the FP32 box
+    // coordinates; the shadow displacement is off by at most ~5 ulp) and the
+    // squares by a relative 2^-20 (three FP32 roundings of r^2 are 2e-7).
+    {
+        const double Lmax = std::max(p.xl[0], std::max(p.xl[1], p.xl[2]));
+        const double delta = Lmax * std::ldexp(1.0, -19);
+        const double grow = 1.0 + std::ldexp(1.0, -20);
+        auto widen2 = [&](double r) {
+            const double rs = (r + delta) * grow;
+            const double r2 = rs * rs * grow;
+            return r2 > 3.0e38 ? INFINITY : (float)r2;
+        };
+        for (int k = 0; k < 3; ++k) {
+            f.Lf[k] = (float)p.xl[k];
+            f.invLf[k] = (float)(1.0 / p.xl[k]);
+        }
+        f.scr_c2 = (p.sim_type == YK_SIM_NUCLEON && !p.coulomb_on) ? -1.0f : widen2(p.rccut);
+        f.scr_n2 = (p.sim_type == YK_SIM_NUCLEON && p.nuclear_on) ? widen2(p.rncut) : -1.0f;
+    }
     f.n = c->n;
     f.nuclear_on = p.nuclear_on;
     f.coulomb_on = p.coulomb_on;
@@ -337,7 +357,8 @@ static int enqueue_order(yk_ctx* c, bool sort)
         ++k;
         c->need_sort = false;
     }
-    k_apply_perm<<<nb, VBLOCK, 0, st>>>(c->perm, c->iperm, c->x, c->zii, c->pos, n, c->sa.pack_w);
+    k_apply_perm<<<nb, VBLOCK, 0, st>>>(c->perm, c->iperm, c->x, c->zii, c->pos, c->posf, n,
+                                        c->sa.pack_w);
     c->pos_dirty = false;
     return k + 1;
 }
@@ -347,7 +368,7 @@ static int launch_force_t(yk_ctx* c)
 {
     if (c->kernel == 1) {
         k_force_rows<SIM, PREC, MEAS><<<c->nfb, FBLOCK, FORCE_SMEM, c->stream>>>(
-            c->pos, c->perm, c->aii, c->fa, c->a, c->fpart, c->err);
+            c->pos, c->posf, c->perm, c->aii, c->fa, c->a, c->fpart, c->err);
         return 1;
     }
     static int grid = 0;
@@ -359,8 +380,8 @@ static int launch_force_t(yk_ctx* c)
     }
     cudaMemsetAsync(c->job_counter, 0, sizeof(int), c->stream);
     const int g = std::min(grid, c->pj.njobs);
-    k_force_pairs<SIM, PREC, MEAS><<<g, PB, 0, c->stream>>>(c->pos, c->pj, c->job_counter, c->fa,
-                                                            c->Si, c->Sj, c->Sm, c->err);
+    k_force_pairs<SIM, PREC, MEAS><<<g, PB, 0, c->stream>>>(c->pos, c->posf, c->pj, c->job_counter,
+                                                            c->fa, c->Si, c->Sj, c->Sm, c->err);
     k_combine<SIM><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->Si, c->Sj, c->pj, c->perm, c->zii,
                                                               c->aii, c->fa, c->a);
     return 2;
@@ -428,9 +449,15 @@ static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool resort, bool t
     cudaStream_t st = c->stream;
     const StepArgs& s = c->sa;
     switch (c->p.integrator) {
-    case YK_VV1: k_drift_vv1<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->iperm, c->pos, s); break;
-    case YK_VV3: k_drift_vv3<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->aii, c->iperm, c->pos, s); break;
-    default: k_drift_vv2<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->vold, c->a, c->zii, c->iperm, c->pos, s); break;
+    case YK_VV1:
+        k_drift_vv1<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->iperm, c->pos, c->posf, s);
+        break;
+    case YK_VV3:
+        k_drift_vv3<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->aii, c->iperm, c->pos, c->posf, s);
+        break;
+    default:
+        k_drift_vv2<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->vold, c->a, c->zii, c->iperm, c->pos, c->posf, s);
+        break;
     }
     ++k;
     k += enqueue_force(c, meas, timed);
@@ -637,7 +664,7 @@ int yk_destroy(yk_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
     free_pairs(c);
-    void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->perm, c->iperm,
+    void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->posf, c->perm, c->iperm,
                     c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->ds, c->err,
                     c->series, c->series_idx, c->job_counter, c->flush_buf};
     for (void* b : bufs) cudaFree(b);
@@ -692,7 +719,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned*)nullptr, (unsigned*)nullptr,
                                     (int*)nullptr, (int*)nullptr, n, 0, 30);
     size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
-                   sizeof(double4) * (size_t)n + sizeof(int) * 5 * (size_t)n + cub_bytes +
+                   (sizeof(double4) + sizeof(float4)) * ((size_t)n + SHADOW_TILE) + sizeof(int) * 5 * (size_t)n + cub_bytes +
                    sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;
     const bool pairs_fit = pair_scratch_bytes(n, c->seg) <= PAIR_SCRATCH_BUDGET;
     if (pairs_fit) bytes += pair_scratch_bytes(n, c->seg);
@@ -720,6 +747,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     ALLOC(c->zii, n);
     ALLOC(c->aii, n);
     ALLOC(c->pos, n);
+    ALLOC(c->posf, (size_t)4 * SHADOW_TILE * ((n + SHADOW_TILE - 1) / SHADOW_TILE));
     ALLOC(c->perm, n);
     ALLOC(c->iperm, n);
     ALLOC(c->keys0, n);
@@ -771,6 +799,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
         for (int i = 0; i < n; ++i) fill[i] = p->ai > 0.0 ? p->ai : 1.0;
         cudaMemcpyAsync(c->aii, fill.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
     }
+    cudaMemsetAsync(c->posf, 0, sizeof(float) * 4 * SHADOW_TILE * ((n + SHADOW_TILE - 1) / SHADOW_TILE), st);
     cudaMemsetAsync(c->ds, 0, sizeof(DevScalars), st);
     cudaMemsetAsync(c->err, 0, sizeof(unsigned), st);
     cudaMemsetAsync(c->series_idx, 0, sizeof(int), st);

@@ -52,8 +52,86 @@ struct ForceArgs {
     double coef;                     // pure: frp zi^2 vc; mix: frp vc; nn: 1
     double xmass, ai_xmass;          // xmass; pure: ai*xmass
     float rc2f, rn2f, xmucf, evcutf, vcf, xpif, xp2if, aaf, aa2f, bpcf, bmcf;
+    // FP32 pre-screen (screen_r2_x2): box, 1/box and squared screening radii
+    // widened by a margin that covers the FP32 rounding of the shadow
+    // positions, so no pair inside a cutoff is ever screened out.
+    float Lf[3], invLf[3];
+    float scr_c2, scr_n2;
     int n, nuclear_on, coulomb_on, mix_compat;
 };
+
+// FP32 shadow positions ("posf") are stored tile by tile in SoA form: tile t
+// (slots 128t .. 128t+127) is a contiguous block of 512 floats x[128], y[128],
+// z[128], w[128], so a source tile is one 2 KB bulk copy and two neighbouring
+// sources' x (y, z) form one aligned float2.
+constexpr int SHADOW_TILE = 128;
+__host__ __device__ __forceinline__ int shadow_index(int slot, int comp)
+{
+    return (slot >> 7) * (4 * SHADOW_TILE) + comp * SHADOW_TILE + (slot & (SHADOW_TILE - 1));
+}
+
+// Target-side constants of the FP32 screen (negated shadow position).
+struct ScreenI {
+    float nx, ny, nz, w;
+};
+
+__device__ __forceinline__ ScreenI load_screen_i(const float* __restrict__ posf, int slot)
+{
+    ScreenI s;
+    s.nx = -posf[shadow_index(slot, 0)];
+    s.ny = -posf[shadow_index(slot, 1)];
+    s.nz = -posf[shadow_index(slot, 2)];
+    s.w = posf[shadow_index(slot, 3)];
+    return s;
+}
+
+// FP32 squared distances from the target to sources j and j+1 of a shadow
+// tile, two at a time with the packed FP32x2 instructions; the minimum image
+// is d - L*rint(d/L) with rint by the 1.5*2^23 magic-number add.  Used only
+// to decide which pairs need the exact FP64 test.
+__device__ __forceinline__ float2 screen_r2_x2(const ForceArgs& fa, const ScreenI& si,
+                                               const float* __restrict__ t, int j)
+{
+    const float2 MAG = make_float2(12582912.0f, 12582912.0f);
+    const float2 NMAG = make_float2(-12582912.0f, -12582912.0f);
+    float2 d[3];
+    const float ni[3] = {si.nx, si.ny, si.nz};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float2 xj = *reinterpret_cast<const float2*>(t + c * SHADOW_TILE + j);
+        float2 dc = __fadd2_rn(xj, make_float2(ni[c], ni[c]));
+        const float2 k = __fadd2_rn(__ffma2_rn(dc, make_float2(fa.invLf[c], fa.invLf[c]), MAG), NMAG);
+        d[c] = __ffma2_rn(make_float2(-fa.Lf[c], -fa.Lf[c]), k, dc);
+    }
+    float2 r2 = __fmul2_rn(d[2], d[2]);
+    r2 = __ffma2_rn(d[1], d[1], r2);
+    return __ffma2_rn(d[0], d[0], r2);
+}
+
+// Scalar form of the same screen for one source j of a shadow tile.
+__device__ __forceinline__ float screen_r2_1(const ForceArgs& fa, const ScreenI& si,
+                                            const float* __restrict__ t, int j)
+{
+    const float MAGIC = 12582912.0f;
+    float dx = t[j] + si.nx, dy = t[SHADOW_TILE + j] + si.ny, dz = t[2 * SHADOW_TILE + j] + si.nz;
+    dx = fmaf(-fa.Lf[0], fmaf(dx, fa.invLf[0], MAGIC) - MAGIC, dx);
+    dy = fmaf(-fa.Lf[1], fmaf(dy, fa.invLf[1], MAGIC) - MAGIC, dy);
+    dz = fmaf(-fa.Lf[2], fmaf(dz, fa.invLf[2], MAGIC) - MAGIC, dz);
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+// Squared screening radius of a pair.  Ions: rccut.  Nucleons: rncut for the
+// nuclear force, or rccut for a p-p pair (Coulomb).
+template <int SIM>
+__device__ __forceinline__ float screen_lim(const ForceArgs& fa, float wi, float wj)
+{
+    if constexpr (SIM == SIM_PURE || SIM == SIM_MIX) {
+        return fa.scr_c2;
+    } else {
+        const bool pp = (wi == 1.0f) && (wj == 1.0f);
+        return (pp && fa.coulomb_on) ? fmaxf(fa.scr_c2, fa.scr_n2) : fa.scr_n2;
+    }
+}
 
 template <typename R>
 struct PairOut {
@@ -285,25 +363,28 @@ __device__ __forceinline__ void store_accel(const ForceArgs& fa, int orig, doubl
     }
 }
 
-// Shared memory of k_force_rows: 2 stages of FTILE double4, 2 mbarriers and
-// the block-reduction scratch.
-constexpr int FORCE_SMEM = 2 * FTILE * (int)sizeof(double4) + 16 + 32 * NSCAL * (int)sizeof(double);
+// Shared memory of k_force_rows: 2 stages of FTILE double4 and one shadow tile,
+// 2 mbarriers and the block-reduction scratch.
+constexpr int FORCE_SMEM = 2 * FTILE * (int)(sizeof(double4) + 4 * sizeof(float)) + 16 +
+                           32 * NSCAL * (int)sizeof(double);
 
 template <int SIM, int PREC, bool MEAS>
 __global__ void __launch_bounds__(FBLOCK)
-k_force_rows(const double4* __restrict__ pos, const int* __restrict__ perm,
-             const double* __restrict__ aii, ForceArgs fa, double* __restrict__ a_out,
-             double* __restrict__ part, unsigned* __restrict__ err)
+k_force_rows(const double4* __restrict__ pos, const float* __restrict__ posf,
+             const int* __restrict__ perm, const double* __restrict__ aii, ForceArgs fa,
+             double* __restrict__ a_out, double* __restrict__ part, unsigned* __restrict__ err)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     double4* tile = reinterpret_cast<double4*>(smem);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * FTILE * sizeof(double4));
-    double* red = reinterpret_cast<double*>(smem + 2 * FTILE * sizeof(double4) + 16);
+    float* tilef = reinterpret_cast<float*>(smem + 2 * FTILE * sizeof(double4));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * FTILE * (sizeof(double4) + 4 * sizeof(float)));
+    double* red = reinterpret_cast<double*>(smem + 2 * FTILE * (sizeof(double4) + 4 * sizeof(float)) + 16);
 
     const int n = fa.n;
     const int i = blockIdx.x * FBLOCK + threadIdx.x;
     const bool active = i < n;
     const double4 pi = active ? pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const ScreenI si = load_screen_i(posf, active ? i : 0);
     const int ntiles = (n + FTILE - 1) / FTILE;
 
     if (threadIdx.x == 0) {
@@ -316,9 +397,11 @@ k_force_rows(const double4* __restrict__ pos, const int* __restrict__ perm,
         const int j0 = t * FTILE;
         const int cnt = min(FTILE, n - j0);
         const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
+        const unsigned bytesf = 4u * SHADOW_TILE * (unsigned)sizeof(float);
         uint64_t* b = &bar[t & 1];
-        mbar_arrive_expect_tx(b, bytes);
+        mbar_arrive_expect_tx(b, bytes + bytesf);
         bulk_g2s(tile + (t & 1) * FTILE, pos + j0, bytes, b);
+        bulk_g2s(tilef + (t & 1) * 4 * SHADOW_TILE, posf + (size_t)t * 4 * SHADOW_TILE, bytesf, b);
     };
     if (threadIdx.x == 0) {
         issue(0);
@@ -342,12 +425,16 @@ k_force_rows(const double4* __restrict__ pos, const int* __restrict__ perm,
         const int j0 = t * FTILE;
         const int cnt = min(FTILE, n - j0);
         const double4* tl = tile + st * FTILE;
+        const float* tlf = tilef + st * 4 * SHADOW_TILE;
         if (active) {
 #pragma unroll 2
             for (int jj = 0; jj < cnt; ++jj) {
-                const double4 pj = tl[jj];
-                pair_eval<SIM, PREC, MEAS>(fa, pi, pj, (j0 + jj) != i, o);
-                if (o.hit) acc.add(o, SIM == SIM_MIX ? (real_t<PREC>)pj.w : (real_t<PREC>)1);
+                if ((j0 + jj) != i &&
+                    screen_r2_1(fa, si, tlf, jj) <= screen_lim<SIM>(fa, si.w, tlf[3 * SHADOW_TILE + jj])) {
+                    const double4 pj = tl[jj];
+                    pair_eval<SIM, PREC, MEAS>(fa, pi, pj, true, o);
+                    if (o.hit) acc.add(o, SIM == SIM_MIX ? (real_t<PREC>)pj.w : (real_t<PREC>)1);
+                }
             }
         }
         __syncthreads();                      // every thread is done with stage st

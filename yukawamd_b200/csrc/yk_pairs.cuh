@@ -11,12 +11,20 @@
 //   job  (R, s)         : units C = R + s*seg ... of one row; persistent CTAs
 //                         pull jobs from an atomic counter (costliest first).
 //
-// Reaction sums: the 4 warps of a CTA sweep the tile in 4 phases, warp w
-// taking the 32-slot chunk (w + phase) mod 4, so every source slot is touched
-// by one warp at a time.  For each source j that any lane hits, the warp sums
-// the 32 reactions with a shuffle butterfly (in FP64 for both forms) and lane
-// 0 adds it to the tile's shared accumulator; phases are separated by CTA
-// barriers, so each accumulator sees its warps in a fixed order.
+// Reaction sums: each warp sweeps the whole tile in groups of 4 sources.  In
+// step jj of a group, lane L takes source jj ^ sw(L), sw(L) = 2*bit4(L) +
+// bit3(L), so its reaction on the group's source sw(L) ends in register slot
+// 0, and the slots that a halving exchange sends are the same for every lane
+// (slots 2,3 over xor 16, then slot 1 over xor 8): the warp sums the 32
+// lanes' reactions on the 4 sources with that reduce-scatter plus a 3-level
+// butterfly (36 shuffles per group instead of 4 x 30, no selects), in FP64
+// for both forms, and lanes 0/8/16/24 add the four sums to the warp's own
+// accumulator row in shared memory.  The 4 warp rows are added in a fixed
+// order at the end of the tile, so no atomics and no per-phase barriers.
+// Every pair is first tested on FP32 shadow positions, two sources per packed
+// FP32x2 instruction (screen_r2_x2); a group none of whose 128 pairs can be
+// inside a cutoff is skipped, and only candidates take the exact FP64
+// minimum-image test and the physics.
 //
 // Outputs are partial sums in scratch (nothing is accumulated atomically):
 //   Si[R][s][PB][3]       target-side sums of job (R, s)
@@ -54,14 +62,94 @@ __device__ __forceinline__ double to_f64(real_t<PREC> v)
     return (double)v;
 }
 
+// Reduce-scatter of four 3-vectors held in lane-swizzled slots (slot q of
+// lane L belongs to source q ^ sw(L)).  On return t[] holds the warp-wide sum
+// for source sw(L).
+__device__ __forceinline__ void reduce_scatter4(double (&r)[4][3], double (&t)[3])
+{
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const double a0 = r[0][c] + __shfl_xor_sync(0xffffffffu, r[2][c], 16);
+        const double a1 = r[1][c] + __shfl_xor_sync(0xffffffffu, r[3][c], 16);
+        t[c] = a0 + __shfl_xor_sync(0xffffffffu, a1, 8);
+    }
+#pragma unroll
+    for (int m = 4; m > 0; m >>= 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t[c] += __shfl_xor_sync(0xffffffffu, t[c], m);
+}
+
+// One group of 4 sources j0..j0+3 for the calling lane's target.  CHECK:
+// the tile is partial, diagonal, or the CTA has inactive targets, so every
+// pair needs the validity test.
+template <int SIM, int PREC, bool MEAS, bool CHECK>
+__device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& pi, const ScreenI& si,
+                                           real_t<PREC> wi, const double4* tl, const float* tlf,
+                                           int j0, int jlim, bool diag, bool active, int tid,
+                                           int sw, TargetAcc<PREC, MEAS>& acc, double* my_acc)
+{
+    using R_t = real_t<PREC>;
+    // screen the 4 sources in natural order, two per packed instruction
+    const float2 ra = screen_r2_x2(fa, si, tlf, j0);
+    const float2 rb = screen_r2_x2(fa, si, tlf, j0 + 2);
+    const float* tw = tlf + 3 * SHADOW_TILE + j0;
+    unsigned m = (ra.x <= screen_lim<SIM>(fa, si.w, tw[0]) ? 1u : 0u) |
+                 (ra.y <= screen_lim<SIM>(fa, si.w, tw[1]) ? 2u : 0u) |
+                 (rb.x <= screen_lim<SIM>(fa, si.w, tw[2]) ? 4u : 0u) |
+                 (rb.y <= screen_lim<SIM>(fa, si.w, tw[3]) ? 8u : 0u);
+    if constexpr (CHECK) {
+        unsigned ok = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int jl = j0 + q;
+            if (active && jl < jlim && (!diag || jl > tid)) ok |= 1u << q;
+        }
+        m &= ok;
+    }
+    if (!__any_sync(0xffffffffu, m != 0)) return;
+    double r[4][3];
+    bool any = false;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+        const int src = jj ^ sw;
+        r[jj][0] = r[jj][1] = r[jj][2] = 0.0;
+        if ((m >> src) & 1u) {
+            const double4 pjv = tl[j0 + src];
+            PairOut<R_t> o;
+            pair_eval<SIM, PREC, MEAS>(fa, pi, pjv, true, o);
+            if (o.hit) {
+                acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
+                // reaction on j: Z_i fs d (int_ion_mix.f:180)
+                const R_t fsj = o.fs * wi;
+                r[jj][0] = to_f64<PREC>(fsj * o.dx);
+                r[jj][1] = to_f64<PREC>(fsj * o.dy);
+                r[jj][2] = to_f64<PREC>(fsj * o.dz);
+                any = true;
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, any)) {
+        double t[3];
+        reduce_scatter4(r, t);
+        const int lane = threadIdx.x & 31;
+        const int jl = j0 + sw;
+        if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
+            my_acc[3 * jl] -= t[0];
+            my_acc[3 * jl + 1] -= t[1];
+            my_acc[3 * jl + 2] -= t[2];
+        }
+    }
+}
+
 template <int SIM, int PREC, bool MEAS>
-__global__ void __launch_bounds__(PB, 4)
-k_force_pairs(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ job_counter,
-              ForceArgs fa, double* __restrict__ Si, double* __restrict__ Sj,
-              double* __restrict__ Sm, unsigned* __restrict__ err)
+__global__ void __launch_bounds__(PB, 5)
+k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, PairJobs pj,
+              int* __restrict__ job_counter, ForceArgs fa, double* __restrict__ Si,
+              double* __restrict__ Sj, double* __restrict__ Sm, unsigned* __restrict__ err)
 {
     __shared__ __align__(128) double4 tile[2][PB];
-    __shared__ double acc_j[PB * 3];
+    __shared__ __align__(128) float tilef[2][4 * SHADOW_TILE];
+    __shared__ double acc_j[PWARPS][PB * 3];
     __shared__ double red[32 * NSCAL];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_job;
@@ -83,9 +171,11 @@ k_force_pairs(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ jo
         const int j0 = C * PB;
         const int cnt = min(PB, n - j0);
         const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
+        const unsigned bytesf = 4u * SHADOW_TILE * (unsigned)sizeof(float);
         uint64_t* b = &bar[qq & 1];
-        mbar_arrive_expect_tx(b, bytes);
+        mbar_arrive_expect_tx(b, bytes + bytesf);
         bulk_g2s(&tile[qq & 1][0], pos + j0, bytes, b);
+        bulk_g2s(&tilef[qq & 1][0], posf + (size_t)C * 4 * SHADOW_TILE, bytesf, b);
     };
 
     for (;;) {
@@ -100,10 +190,11 @@ k_force_pairs(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ jo
         const int i = R * PB + tid;
         const bool active = i < n;
         const double4 pi = active ? pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        const ScreenI si = load_screen_i(posf, active ? i : 0);
         const R_t wi = (SIM == SIM_MIX) ? (R_t)pi.w : (R_t)1;   // Z_i of the reaction
+        const bool all_active = (R + 1) * PB <= n;
         TargetAcc<PREC, MEAS> acc;
         acc.zero();
-        PairOut<R_t> o;
 
         if (tid == 0) {
             issue(C0, q);
@@ -111,9 +202,12 @@ k_force_pairs(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ jo
         }
         for (int C = C0; C < C1; ++C, ++q) {
             const int st = q & 1;
-            acc_j[3 * tid] = 0.0;
-            acc_j[3 * tid + 1] = 0.0;
-            acc_j[3 * tid + 2] = 0.0;
+#pragma unroll
+            for (int w = 0; w < PWARPS; ++w) {
+                acc_j[w][3 * tid] = 0.0;
+                acc_j[w][3 * tid + 1] = 0.0;
+                acc_j[w][3 * tid + 2] = 0.0;
+            }
             const bool ok = mbar_wait_bounded(&bar[st], (q >> 1) & 1u, err);
             if (__syncthreads_or(!ok)) {
                 if (tid == 0 && C + 1 < C1) mbar_wait_bounded(&bar[st ^ 1], ((q + 1) >> 1) & 1u, err);
@@ -122,44 +216,28 @@ k_force_pairs(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ jo
             const int jlim = min(PB, n - C * PB);
             const bool diag = (C == R);
             const double4* tl = tile[st];
-#pragma unroll 1
-            for (int ph = 0; ph < PWARPS; ++ph) {
-                const int jb = ((warp + ph) & (PWARPS - 1)) * 32;
-                const int je = min(jb + 32, jlim);
-                for (int jl = jb; jl < je; ++jl) {
-                    const double4 pjv = tl[jl];
-                    const bool valid = active && (!diag || jl > tid);
-                    pair_eval<SIM, PREC, MEAS>(fa, pi, pjv, valid, o);
-                    if (o.hit) acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
-                    if (__any_sync(0xffffffffu, o.hit)) {
-                        // reaction on j: sum over the warp of Z_i fs d (int_ion_mix.f:180)
-                        double rx = 0.0, ry = 0.0, rz = 0.0;
-                        if (o.hit) {
-                            const R_t fsj = o.fs * wi;
-                            rx = to_f64<PREC>(fsj * o.dx);
-                            ry = to_f64<PREC>(fsj * o.dy);
-                            rz = to_f64<PREC>(fsj * o.dz);
-                        }
-#pragma unroll
-                        for (int m = 16; m > 0; m >>= 1) {
-                            rx += __shfl_xor_sync(0xffffffffu, rx, m);
-                            ry += __shfl_xor_sync(0xffffffffu, ry, m);
-                            rz += __shfl_xor_sync(0xffffffffu, rz, m);
-                        }
-                        if (lane == 0) {
-                            acc_j[3 * jl] -= rx;
-                            acc_j[3 * jl + 1] -= ry;
-                            acc_j[3 * jl + 2] -= rz;
-                        }
-                    }
-                }
-                __syncthreads();
+            const float* tlf = tilef[st];
+            double* my_acc = acc_j[warp];
+            const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
+            if (!diag && jlim == PB && all_active) {
+                for (int j0 = 0; j0 < PB; j0 += 4)
+                    pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active,
+                                                       tid, sw, acc, my_acc);
+            } else {
+                for (int j0 = 0; j0 < jlim; j0 += 4)
+                    pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active,
+                                                      tid, sw, acc, my_acc);
             }
-            // source-side partial of unit (R, C)
+            __syncthreads();
+            // source-side partial of unit (R, C): the warp rows in fixed order
             double* dj = Sj + ((size_t)tri_index(C, R) * PB + tid) * 3;
-            dj[0] = acc_j[3 * tid];
-            dj[1] = acc_j[3 * tid + 1];
-            dj[2] = acc_j[3 * tid + 2];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double v = acc_j[0][3 * tid + c];
+#pragma unroll
+                for (int w = 1; w < PWARPS; ++w) v += acc_j[w][3 * tid + c];
+                dj[c] = v;
+            }
             __syncthreads();                  // stage st and acc_j are free again
             if (tid == 0 && C + 2 < C1) issue(C + 2, q + 2);
         }

@@ -10,7 +10,7 @@
 // keeps the permutation a deterministic function of the positions.
 #pragma once
 
-#include "yk_common.cuh"
+#include "yk_force.cuh"
 
 namespace yk {
 
@@ -40,13 +40,19 @@ __global__ void k_morton(const double* __restrict__ x, int n, double sx, double 
 // Slot s holds particle perm[s]; iperm is the inverse; pos is repacked.
 __global__ void k_apply_perm(const int* __restrict__ perm, int* __restrict__ iperm,
                              const double* __restrict__ x, const double* __restrict__ zii,
-                             double4* __restrict__ pos, int n, int pack_w)
+                             double4* __restrict__ pos, float* __restrict__ posf, int n,
+                             int pack_w)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const int o = perm[s];
     iperm[o] = s;
-    pos[s] = make_double4(x[3 * o], x[3 * o + 1], x[3 * o + 2], pack_w ? zii[o] : 0.0);
+    const double4 p = make_double4(x[3 * o], x[3 * o + 1], x[3 * o + 2], pack_w ? zii[o] : 0.0);
+    pos[s] = p;
+    posf[shadow_index(s, 0)] = (float)p.x;
+    posf[shadow_index(s, 1)] = (float)p.y;
+    posf[shadow_index(s, 2)] = (float)p.z;
+    posf[shadow_index(s, 3)] = (float)p.w;
 }
 
 }  // namespace yk

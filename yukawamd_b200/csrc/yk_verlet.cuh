@@ -16,7 +16,7 @@
 // kernels stream (slot iperm[i] for particle i).
 #pragma once
 
-#include "yk_common.cuh"
+#include "yk_force.cuh"
 
 namespace yk {
 
@@ -40,6 +40,17 @@ __device__ __forceinline__ double wrap_once(double x, double L)
     return x;
 }
 
+// Slot `slot` of the FP64 positions and of their FP32 shadow (screening).
+__device__ __forceinline__ void store_pos(double4* pos, float* posf, int slot, const double (&xn)[3],
+                                          double w)
+{
+    pos[slot] = make_double4(xn[0], xn[1], xn[2], w);
+    posf[shadow_index(slot, 0)] = (float)xn[0];
+    posf[shadow_index(slot, 1)] = (float)xn[1];
+    posf[shadow_index(slot, 2)] = (float)xn[2];
+    posf[shadow_index(slot, 3)] = (float)w;
+}
+
 // x = x + v dt + afac a, wrapped once (vel_verlet_2.f:36-42)
 __device__ __forceinline__ double drift1(double x, double v, double a, const StepArgs& s, int k)
 {
@@ -49,7 +60,8 @@ __device__ __forceinline__ double drift1(double x, double v, double a, const Ste
 // VV2 first half: drift, vold = v, v += dt a.
 __global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold,
                             const double* __restrict__ a, const double* __restrict__ zii,
-                            const int* __restrict__ iperm, double4* __restrict__ pos, StepArgs s)
+                            const int* __restrict__ iperm, double4* __restrict__ pos,
+                            float* __restrict__ posf, StepArgs s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
@@ -63,13 +75,14 @@ __global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, doub
         vold[e] = vi;
         v[e] = __dadd_rn(vi, __dmul_rn(s.dt, ai));
     }
-    pos[iperm[i]] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
+    store_pos(pos, posf, iperm[i], xn, s.pack_w ? zii[i] : 0.0);
 }
 
 // VV1 first half: drift, v += dt/2 a (vel_verlet_1.f:148-166).
 __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
                             const double* __restrict__ a, const double* __restrict__ zii,
-                            const int* __restrict__ iperm, double4* __restrict__ pos, StepArgs s)
+                            const int* __restrict__ iperm, double4* __restrict__ pos,
+                            float* __restrict__ posf, StepArgs s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
@@ -82,7 +95,7 @@ __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
         x[e] = xn[k];
         v[e] = __dadd_rn(v[e], __dmul_rn(s.halfdt, ai));
     }
-    pos[iperm[i]] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
+    store_pos(pos, posf, iperm[i], xn, s.pack_w ? zii[i] : 0.0);
 }
 
 // VV3 first half: drift and the first Spreiter-Walter stage
@@ -90,7 +103,7 @@ __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
 __global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ v,
                             const double* __restrict__ a, const double* __restrict__ zii,
                             const double* __restrict__ aii, const int* __restrict__ iperm,
-                            double4* __restrict__ pos, StepArgs s)
+                            double4* __restrict__ pos, float* __restrict__ posf, StepArgs s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
@@ -114,7 +127,7 @@ __global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ v,
     v[3 * i] = v1;
     v[3 * i + 1] = v2;
     v[3 * i + 2] = v3;
-    pos[iperm[i]] = make_double4(xn[0], xn[1], xn[2], s.pack_w ? zii[i] : 0.0);
+    store_pos(pos, posf, iperm[i], xn, s.pack_w ? zii[i] : 0.0);
 }
 
 template <bool KIN>
