@@ -209,6 +209,29 @@ YK_API int yk_perf_read(yk_ctx* ctx, yk_perf* out);
  * over the whole GPU.  Used for roofline denominators. */
 YK_API int yk_peak_probe(int device, int kind, double* tflops);
 
+/*
+ * Force call that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when
+ * they need forces -- code running while a stream is captured into a CUDA
+ * graph (cudaMalloc is not allowed there) or applications whose own pool
+ * allocator owns all device memory.  It computes what yk_accel computes, for
+ * one box given entirely by caller-owned DEVICE arrays: x_dev double[3n],
+ * zii_dev / aii_dev double[n] (NULL allowed where yk_create allows NULL),
+ * a_dev double[3(n+3)] (output, same layout as yk_accel's a_out).  out (host)
+ * may be NULL; stream may be NULL (legacy default stream).  The call waits
+ * for its stream before returning.
+ *
+ * Limits: n <= 4096.  Working memory is one fixed 4 MiB array in the
+ * library's device code, held by every GPU that loads the library until the
+ * process exits.  The first call on a device looks up that array's address;
+ * make that first call before starting any stream capture.  Every call reuses
+ * the same array, so calls that overlap on the GPU race: serialise them.
+ */
+YK_API int yk_accel_noalloc(const yk_params* p, int n,
+                            const double* x_dev, const double* zii_dev,
+                            const double* aii_dev, int do_meas,
+                            double* a_dev, yk_scalars* out, void* stream);
+
 /* Page-lock a caller-owned host buffer so that yk_get_state / yk_set_state
  * copy it by DMA.  Optional. */
 YK_API int yk_host_register(void* ptr, size_t bytes);

@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1078,3 +1079,236 @@ int yk_host_unregister(void* ptr)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Force call without device allocation (yk_accel_noalloc).
+//
+// Some callers cannot allocate device memory at the moment they need forces:
+// code that runs while a stream is being captured into a CUDA graph (where
+// cudaMalloc is not permitted), or applications that hand every byte of
+// device memory to their own pool allocator and forbid allocations behind
+// its back.  For them this entry point evaluates one force call on
+// caller-owned device arrays and keeps all of its working memory -- packed
+// positions, their FP32 shadow, the slot order, the job table and the
+// partial sums of the half-pair kernel -- in the file-scope array below.
+// The array is created when the library's device code is loaded and stays
+// on every GPU that loaded it until the process exits.  It caps n at
+// NOALLOC_MAX_N; larger calls are rejected.  All calls share the array: two
+// calls that overlap on the GPU (different streams, or different host
+// threads on one device) race and corrupt each other's results.
+
+constexpr int NOALLOC_MAX_N = 4096;
+constexpr int NOALLOC_SEG = 4;
+constexpr size_t NOALLOC_BYTES = size_t(4) << 20;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+// Device address of g_noalloc_scratch per device, looked up on the first call
+// on that device (with the device current).
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static void* g_noalloc_addr[NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mutex;
+
+__global__ void k_noalloc_prepare(int* perm, int n, int2* jobs, int M, int seg)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) perm[s] = s;                      // slots in the caller's order
+    if (s == 0) {
+        int k = 0;
+        for (int R = 0; R < M; ++R)
+            for (int q = 0; q * seg < M - R; ++q) jobs[k++] = make_int2(R, q);
+    }
+}
+
+// Byte layout of the scratch for n particles (256-byte aligned pieces).
+struct NoallocLayout {
+    size_t pos, posf, perm, iperm, Si, Sj, Sm, jobs, ds, counter, err, total;
+    int M, nseg, njobs;
+};
+
+static NoallocLayout noalloc_layout(int n)
+{
+    NoallocLayout L{};
+    L.M = (n + PB - 1) / PB;
+    L.nseg = (L.M + NOALLOC_SEG - 1) / NOALLOC_SEG;
+    L.njobs = 0;
+    for (int R = 0; R < L.M; ++R) L.njobs += (L.M - R + NOALLOC_SEG - 1) / NOALLOC_SEG;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = off;
+        off += (bytes + 255) & ~size_t(255);
+        return at;
+    };
+    L.pos = take(sizeof(double4) * (size_t)n);
+    L.posf = take(sizeof(float) * 4 * SHADOW_TILE * (size_t)L.M);
+    L.perm = take(sizeof(int) * (size_t)n);
+    L.iperm = take(sizeof(int) * (size_t)n);
+    L.Si = take(sizeof(double) * 3 * PB * (size_t)L.M * L.nseg);
+    L.Sj = take(sizeof(double) * 3 * PB * ((size_t)L.M * (L.M + 1) / 2));
+    L.Sm = take(sizeof(double) * NSCAL * (size_t)L.njobs);
+    L.jobs = take(sizeof(int2) * (size_t)L.njobs);
+    L.ds = take(sizeof(DevScalars));
+    L.counter = take(sizeof(int));
+    L.err = take(sizeof(unsigned));
+    L.total = off;
+    return L;
+}
+
+template <int SIM, int PREC, bool MEAS>
+static void noalloc_force(cudaStream_t st, const double4* pos, const float* posf, PairJobs pj, int* counter,
+                          const ForceArgs& fa, double* Si, double* Sj, double* Sm, unsigned* err,
+                          const int* perm, const double* zii, const double* aii, double* a)
+{
+    static int grid = 0;
+    if (grid == 0) {
+        int per_sm = 0, sms = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs<SIM, PREC, MEAS>, PB, 0);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        grid = std::max(1, per_sm) * std::max(1, sms);
+    }
+    k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter, fa, Si, Sj,
+                                                                            Sm, err);
+    k_combine<SIM><<<(fa.n + 255) / 256, 256, 0, st>>>(Si, Sj, pj, perm, zii, aii, fa, a);
+}
+
+template <int SIM>
+static void noalloc_force_s(bool mixed, bool meas, cudaStream_t st, const double4* pos, const float* posf,
+                            PairJobs pj, int* counter, const ForceArgs& fa, double* Si, double* Sj,
+                            double* Sm, unsigned* err, const int* perm, const double* zii,
+                            const double* aii, double* a)
+{
+    if (mixed) {
+        if (meas) noalloc_force<SIM, PREC_MIXED, true>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+        else noalloc_force<SIM, PREC_MIXED, false>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+    } else {
+        if (meas) noalloc_force<SIM, PREC_FP64, true>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+        else noalloc_force<SIM, PREC_FP64, false>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+    }
+}
+
+extern "C" int yk_accel_noalloc(const yk_params* p, int n, const double* x_dev, const double* zii_dev,
+                                const double* aii_dev, int do_meas, double* a_dev, yk_scalars* out,
+                                void* stream)
+{
+    if (!p || !x_dev || !a_dev) return fail(nullptr, YK_ERR_ARG, "params, x and a are required");
+    if (n < 1) return fail(nullptr, YK_ERR_ARG, "n must be >= 1 (got %d)", n);
+    if (n > NOALLOC_MAX_N)
+        return fail(nullptr, YK_ERR_ARG,
+                    "yk_accel_noalloc handles at most n = %d particles (got %d); use yk_create/yk_accel",
+                    NOALLOC_MAX_N, n);
+    int rc = check_params(p);
+    if (rc) return rc;
+    if ((p->sim_type == YK_SIM_ION_MIXTURE || p->sim_type == YK_SIM_NUCLEON) && !zii_dev)
+        return fail(nullptr, YK_ERR_ARG, "this sim_type needs zii");
+    if (p->sim_type == YK_SIM_ION_MIXTURE && !aii_dev)
+        return fail(nullptr, YK_ERR_ARG, "ion-mixture runs need aii");
+    const NoallocLayout L = noalloc_layout(n);
+    if (L.total > NOALLOC_BYTES)
+        return fail(nullptr, YK_ERR_ARG, "n = %d needs %zu scratch bytes, more than the %zu available", n,
+                    L.total, NOALLOC_BYTES);
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(nullptr, YK_ERR_CUDA, "cudaGetDevice failed");
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(nullptr, YK_ERR_ARG, "device %d not supported", dev);
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_addr[dev]) {
+            // first call on this device: device-side address of the array
+            cudaError_t e = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_noalloc_addr[dev] = nullptr;
+                return fail(nullptr, YK_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            }
+        }
+        base = g_noalloc_addr[dev];
+    }
+    unsigned char* b = static_cast<unsigned char*>(base);
+    double4* pos = reinterpret_cast<double4*>(b + L.pos);
+    float* posf = reinterpret_cast<float*>(b + L.posf);
+    int* perm = reinterpret_cast<int*>(b + L.perm);
+    int* iperm = reinterpret_cast<int*>(b + L.iperm);
+    double* Si = reinterpret_cast<double*>(b + L.Si);
+    double* Sj = reinterpret_cast<double*>(b + L.Sj);
+    double* Sm = reinterpret_cast<double*>(b + L.Sm);
+    int2* jobs = reinterpret_cast<int2*>(b + L.jobs);
+    DevScalars* ds = reinterpret_cast<DevScalars*>(b + L.ds);
+    int* counter = reinterpret_cast<int*>(b + L.counter);
+    unsigned* err = reinterpret_cast<unsigned*>(b + L.err);
+
+    // argument blocks from the same builder the engine uses (no allocation)
+    yk_ctx tmp;
+    tmp.p = *p;
+    tmp.n = n;
+    setup_args(&tmp);
+    const ForceArgs& fa = tmp.fa;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool meas = do_meas != 0;
+
+    // clear what must start at zero: shadow padding, scalars, counter, error word
+    CK(nullptr, cudaMemsetAsync(posf, 0, sizeof(float) * 4 * SHADOW_TILE * (size_t)L.M, st));
+    CK(nullptr, cudaMemsetAsync(ds, 0, sizeof(DevScalars), st));
+    CK(nullptr, cudaMemsetAsync(counter, 0, sizeof(int), st));
+    CK(nullptr, cudaMemsetAsync(err, 0, sizeof(unsigned), st));
+    k_noalloc_prepare<<<(n + 255) / 256, 256, 0, st>>>(perm, n, jobs, L.M, NOALLOC_SEG);
+    k_apply_perm<<<(n + VBLOCK - 1) / VBLOCK, VBLOCK, 0, st>>>(perm, iperm, x_dev, zii_dev, pos, posf, n,
+                                                              tmp.sa.pack_w);
+    int k = 2;
+    PairJobs pj{};
+    pj.jobs = jobs;
+    pj.njobs = L.njobs;
+    pj.M = L.M;
+    pj.seg = NOALLOC_SEG;
+    pj.nseg_max = L.nseg;
+    const bool mixed = p->precision == YK_PREC_MIXED;
+    switch (p->sim_type) {
+    case YK_SIM_PURE_ION:
+        noalloc_force_s<SIM_PURE>(mixed, meas, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii_dev,
+                                  aii_dev, a_dev);
+        k += 2;
+        break;
+    case YK_SIM_ION_MIXTURE:
+        noalloc_force_s<SIM_MIX>(mixed, meas, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii_dev,
+                                 aii_dev, a_dev);
+        k += 2;
+        break;
+    case YK_SIM_NUCLEON:
+        noalloc_force_s<SIM_NUCLEON>(mixed, meas, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm,
+                                     zii_dev, aii_dev, a_dev);
+        k += 2;
+        break;
+    default:  // 'B-field': a = 0
+        CK(nullptr, cudaMemsetAsync(a_dev, 0, sizeof(double) * 3 * (size_t)(n + 3), st));
+        break;
+    }
+    FinishArgs z = tmp.fz_base;
+    const bool has_force = p->sim_type != YK_SIM_BFIELD;
+    z.force_mode = has_force ? 1 : 0;
+    z.do_meas = meas ? 1 : 0;
+    z.nfp = (has_force && meas) ? L.njobs : 0;
+    z.half = 1.0;
+    z.kin_mode = 0;
+    z.nkp = 0;
+    k_finish<<<1, 256, 0, st>>>(Sm, nullptr, z, a_dev, ds, nullptr, nullptr);
+    ++k;
+    g_launches += k;
+
+    DevScalars h{};
+    unsigned herr = 0;
+    CK(nullptr, cudaMemcpyAsync(&h, ds, sizeof h, cudaMemcpyDeviceToHost, st));
+    CK(nullptr, cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, st));
+    CK(nullptr, cudaStreamSynchronize(st));
+    CK(nullptr, cudaGetLastError());
+    if (herr) return fail(nullptr, (herr & ERR_TIMEOUT) ? YK_ERR_TIMEOUT : YK_ERR_CUDA,
+                          "device error word 0x%x", herr);
+    if (out) {
+        out->ev = h.ev;
+        out->vir = h.vir;
+        out->px = h.px;
+        out->ek = h.ek;
+        for (int q = 0; q < 9; ++q) out->pp[q] = h.pp[q];
+        out->time = p->time;
+    }
+    return YK_OK;
+}

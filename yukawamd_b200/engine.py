@@ -172,6 +172,17 @@ def peak_probe(device=0, kind=0):
     return out.value
 
 
+def accel_noalloc(params, n, x_dev, zii_dev, aii_dev, do_measurements, a_dev, stream=None):
+    """Force call on caller-owned device arrays (raw device addresses as ints)
+    that allocates no device memory; see yk_accel_noalloc in
+    include/yukawa_engine.h for who needs it and its limits (n <= 4096, calls
+    must not overlap on the GPU).  Returns the scalars."""
+    out = abi.YkScalars()
+    check(lib().yk_accel_noalloc(C.byref(params), int(n), x_dev, zii_dev, aii_dev,
+                                 int(bool(do_measurements)), a_dev, C.byref(out), stream))
+    return out
+
+
 def version():
     return lib().yk_version().decode()
 
