@@ -210,6 +210,7 @@ def time_engine(w, precision, steps, warmup, meas_every, dist, flush=True):
     from yukawamd_b200.engine import Engine, kernel_launch_count
     prec = abi.YK_PREC_MIXED if precision == "mixed" else abi.YK_PREC_FP64
     e = Engine(w, precision=prec, device=dist.local)
+    e.kernel_name = {1: "k_force_rows", 2: "k_force_pairs"}.get(e.tuning().force_kernel, "?")
     e.accel(True)                                  # md.F:69, initial forces
     if warmup:
         e.run(warmup, meas_every, series=False)
@@ -257,17 +258,22 @@ def e2e_engine(w, steps, warmup, meas_every, dist):
     return (t1 - t0) * 1e3, 2 * 24 * w.n, 2 * 24 * w.n + 112
 
 
-def read_traffic(kernel_tag):
-    """DRAM bytes per force launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "force_%s.md" % kernel_tag)
-    if not os.path.exists(path):
+def read_traffic(kind, precision):
+    """DRAM bytes per force launch from the committed ncu summaries
+    (a line "traffic_bytes_per_launch <kind> <precision>: <bytes>")."""
+    key = "traffic_bytes_per_launch %s %s:" % (kind, precision)
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
         return None
-    for line in open(path):
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
+    for name in sorted(os.listdir(pdir)):
+        if not name.endswith(".md"):
+            continue
+        for line in open(os.path.join(pdir, name)):
+            if line.startswith(key):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
     return None
 
 
@@ -325,12 +331,11 @@ def run_ours(args, dist):
     prec_kind = 1 if args.precision == "mixed" else 0
     peak = peak_probe(dist.local, prec_kind)
     achieved = fpp * pairs_step / (force_ms * 1e-3) / 1e12
-    tag = "%s_%s" % (kind, args.precision)
     roofline = {"bound": "fp64" if prec_kind == 0 else "fp32", "achieved": achieved,
                 "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": read_traffic(tag),
-                "kernel": "k_force_rows (force kernel), avg %.3f ms/launch over %d launches"
-                          % (force_ms, perf.force_calls),
+                "traffic": read_traffic(kind, args.precision),
+                "kernel": "%s + k_combine (force call), avg %.3f ms/launch over %d launches"
+                          % (e.kernel_name, force_ms, perf.force_calls),
                 "peak_source": "measured live by yk_peak_probe (%s FMA chain, all SMs)"
                                % ("FP64" if prec_kind == 0 else "FP32"),
                 "flops_per_pair": fpp, "force_share_of_step": perf.force_ms / perf.run_ms}

@@ -176,7 +176,8 @@ YK_API int yk_set_box(yk_ctx* ctx, const double xl[3]);
  */
 typedef struct yk_tuning {
     int force_kernel;     /* 0 auto, 1 row kernel (each pair from both sides),
-                             2 half-pair kernel (Newton's third law, scratch)  */
+                             2 half-pair kernel (Newton's third law, scratch);
+                             yk_get_tuning reports the kernel auto resolved to */
     int pair_seg;         /* source tiles per job of the half-pair kernel     */
     int sort_every;       /* steps between Morton re-orderings (-1 = never)   */
     int graph_steps;      /* steps captured per CUDA graph by yk_run          */

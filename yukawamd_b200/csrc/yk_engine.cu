@@ -817,7 +817,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
 int yk_get_tuning(yk_ctx* c, yk_tuning* out)
 {
     if (!c || !out) return fail(c, YK_ERR_ARG, "ctx and out are required");
-    out->force_kernel = c->kernel_req == 0 ? 0 : c->kernel;
+    out->force_kernel = c->kernel;          // the resolved kernel (1 rows, 2 pairs)
     out->pair_seg = c->seg;
     out->sort_every = c->sort_every;
     out->graph_steps = c->graph_steps;

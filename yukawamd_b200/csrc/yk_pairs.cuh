@@ -149,7 +149,7 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
 {
     __shared__ __align__(128) double4 tile[2][PB];
     __shared__ __align__(128) float tilef[2][4 * SHADOW_TILE];
-    __shared__ double acc_j[PWARPS][PB * 3];
+    __shared__ double acc_j[2][PWARPS][PB * 3];    // double-buffered by tile
     __shared__ double red[32 * NSCAL];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_job;
@@ -202,11 +202,13 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
         }
         for (int C = C0; C < C1; ++C, ++q) {
             const int st = q & 1;
+            // zero this tile's accumulator rows; the other buffer may still
+            // be read by threads finishing the previous tile's sum
 #pragma unroll
             for (int w = 0; w < PWARPS; ++w) {
-                acc_j[w][3 * tid] = 0.0;
-                acc_j[w][3 * tid + 1] = 0.0;
-                acc_j[w][3 * tid + 2] = 0.0;
+                acc_j[st][w][3 * tid] = 0.0;
+                acc_j[st][w][3 * tid + 1] = 0.0;
+                acc_j[st][w][3 * tid + 2] = 0.0;
             }
             const bool ok = mbar_wait_bounded(&bar[st], (q >> 1) & 1u, err);
             if (__syncthreads_or(!ok)) {
@@ -217,7 +219,7 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
             const bool diag = (C == R);
             const double4* tl = tile[st];
             const float* tlf = tilef[st];
-            double* my_acc = acc_j[warp];
+            double* my_acc = acc_j[st][warp];
             const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
             if (!diag && jlim == PB && all_active) {
                 for (int j0 = 0; j0 < PB; j0 += 4)
@@ -228,18 +230,17 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
                     pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active,
                                                       tid, sw, acc, my_acc);
             }
-            __syncthreads();
+            __syncthreads();                  // tile done: stage st reusable, rows complete
+            if (tid == 0 && C + 2 < C1) issue(C + 2, q + 2);
             // source-side partial of unit (R, C): the warp rows in fixed order
             double* dj = Sj + ((size_t)tri_index(C, R) * PB + tid) * 3;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                double v = acc_j[0][3 * tid + c];
+                double v = acc_j[st][0][3 * tid + c];
 #pragma unroll
-                for (int w = 1; w < PWARPS; ++w) v += acc_j[w][3 * tid + c];
+                for (int w = 1; w < PWARPS; ++w) v += acc_j[st][w][3 * tid + c];
                 dj[c] = v;
             }
-            __syncthreads();                  // stage st and acc_j are free again
-            if (tid == 0 && C + 2 < C1) issue(C + 2, q + 2);
         }
         // target-side partial of job (R, s)
         double* di = Si + (((size_t)R * pj.nseg_max + sg) * PB + tid) * 3;
