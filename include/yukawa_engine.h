@@ -170,6 +170,41 @@ YK_API int yk_set_state(yk_ctx* ctx, const double* x, const double* v,
 YK_API int yk_set_box(yk_ctx* ctx, const double xl[3]);
 
 /*
+ * Batches of independent boxes.  The reference runs one box per process; the
+ * engine can also advance many boxes together (ensembles, served requests):
+ * one persistent force kernel pulls (box, target block, source segment)
+ * work items of all boxes from one queue, the integrator kernels cover all
+ * boxes per launch, and yk_batch_run captures K steps of all boxes in one
+ * CUDA graph.  Each box keeps its own parameters, N, state and scalars, and
+ * its results do not depend on which other boxes share the batch.
+ *
+ * A batch holds either ion boxes (pure-ion and ion-mixture; pure-ion boxes
+ * run through the mixture kernels with every Z equal to zi) or nucleon
+ * boxes, all with one precision, integrator YK_VV2 and no B field.  Per-box
+ * arrays are passed as arrays of pointers: x[r] double[3 n[r]], v[r] (or
+ * NULL), zii[r] / aii[r] (NULL allowed where yk_create allows it).
+ */
+typedef struct yk_batch yk_batch;
+
+YK_API int yk_batch_create(int nrep, const yk_params* params, const int* n,
+                           const double* const* x, const double* const* v,
+                           const double* const* zii, const double* const* aii,
+                           int device, yk_batch** out);
+YK_API int yk_batch_destroy(yk_batch* b);
+YK_API const char* yk_batch_last_error(const yk_batch* b);
+/* accel(do_meas) of every box; out: nrep scalars or NULL. */
+YK_API int yk_batch_accel(yk_batch* b, int do_meas, yk_scalars* out);
+/* nsteps newton steps of every box; step s (1-based) measures when
+ * meas_every > 0 and s % meas_every == 0.  series: nsteps*nrep scalars,
+ * step-major (series[s*nrep + r]) or NULL.  ms: CUDA-event time of the
+ * device work or NULL. */
+YK_API int yk_batch_run(yk_batch* b, int nsteps, int meas_every,
+                        yk_scalars* series, double* ms);
+/* State of box rep: x, v, vold double[3 n[rep]]; a double[3(n[rep]+3)]. */
+YK_API int yk_batch_get_state(yk_batch* b, int rep, double* x, double* v,
+                              double* vold, double* a);
+
+/*
  * Engine tunables (not reference parameters): which force kernel runs and
  * how its work is cut.  yk_create picks defaults; the autotuner
  * (yukawamd_b200/tune.py) measures the alternatives and sets them here.

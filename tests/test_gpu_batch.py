@@ -1,0 +1,101 @@
+"""Batches of independent boxes (yk_batch_*) through the C-ABI.
+
+Each box of a batch must give what the single-box engine gives (FP64:
+2-norm relative 1e-12; the batch runs pure-ion boxes through the mixture
+kernels, which changes only rounding) and must give bit-identical results
+whether it runs alone or among other boxes, because its work items write only
+its own scratch rows and its slot order depends only on its own positions.
+"""
+import numpy as np
+import pytest
+
+from yukawamd_b200 import abi, configs
+from yukawamd_b200.engine import Batch, Engine
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def ion_boxes():
+    return [configs.pure_ion(700, 8, 16, 1.0, 175.0, seed=1),
+            configs.ion_mixture(1500, [6, 8, 26], [0.2, 0.7, 0.1], 0.5, 150.0, seed=2),
+            configs.pure_ion(129, 26, 52, 2.0, 60.0, seed=3),
+            configs.ion_mixture(3001, [6, 8], [0.5, 0.5], 1.2, 90.0, seed=4),
+            configs.pure_ion(1, 6, 12, 1.0, 100.0, seed=5)]
+
+
+def nucleon_boxes():
+    return [configs.nucleon(800, 0.4, 0.05, 1.0, 10.0, 2.0, seed=6),
+            configs.nucleon(2000, 0.3, 0.05, 1.0, 10.0, 2.0, seed=7)]
+
+
+@pytest.mark.parametrize("prec,tol", [(abi.YK_PREC_FP64, 1e-12), (abi.YK_PREC_MIXED, 1e-6)],
+                         ids=["fp64", "mixed"])
+@pytest.mark.parametrize("kind", ["ion", "nucleon"])
+def test_batch_accel_matches_single_boxes(gpu, kind, prec, tol):
+    boxes = ion_boxes() if kind == "ion" else nucleon_boxes()
+    with Batch(boxes, precision=prec, mix_mode=abi.YK_MIX_FIXED) as b:
+        sc = b.accel(True)
+        states = [b.get_state(r) for r in range(b.nrep)]
+    for r, w in enumerate(boxes):
+        fixed = abi.YK_MIX_FIXED
+        with Engine(w, precision=prec, mix_mode=fixed) as e:
+            s = e.accel(True)
+            a = e.a.copy()
+        n = w.n
+        ab = states[r][3]
+        if n > 1:
+            assert _rel(ab[:3 * n], a[:3 * n]) <= tol, (kind, r)
+            assert _rel(ab[3 * n:], a[3 * n:]) <= max(tol, 1e-12), (kind, r)
+            assert abs(sc[r].ev - s.ev) <= tol * abs(s.ev)
+            assert abs(sc[r].px - s.px) <= tol * abs(s.px)
+
+
+def test_batch_steps_match_single_boxes(gpu):
+    boxes = ion_boxes()[:4]
+    steps, me = 60, 10
+    with Batch(boxes, mix_mode=abi.YK_MIX_FIXED) as b:
+        b.accel(True)
+        ser, ms = b.run(steps, me)
+        states = [b.get_state(r) for r in range(b.nrep)]
+    assert ms > 0.0
+    for r, w in enumerate(boxes):
+        with Engine(w, mix_mode=abi.YK_MIX_FIXED) as e:
+            e.accel(True)
+            s1 = e.run(steps, me)
+            x, v, _, _ = e.get_state()
+        assert _rel(states[r][0], x) <= 1e-12
+        assert _rel(states[r][1], v) <= 1e-9
+        last = ser[(steps - 1) * b.nrep + r]
+        assert abs(last.ev - s1[steps - 1].ev) <= 1e-9 * abs(s1[steps - 1].ev)
+        assert abs(last.ek - s1[steps - 1].ek) <= 1e-9 * abs(s1[steps - 1].ek)
+        assert last.time == s1[steps - 1].time
+
+
+@pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
+def test_box_alone_equals_box_in_the_mix(gpu, prec):
+    boxes = ion_boxes()
+    target = 3
+    steps = 73
+    with Batch(boxes, precision=prec) as b:
+        b.accel(True)
+        ser_mix, _ = b.run(steps, 7)
+        st_mix = b.get_state(target)
+    with Batch([boxes[target]], precision=prec) as b1:
+        b1.accel(True)
+        ser_one, _ = b1.run(steps, 7)
+        st_one = b1.get_state(0)
+    for A, B in zip(st_mix, st_one):
+        assert np.array_equal(A, B)
+    for s in range(steps):
+        assert bytes(ser_mix[s * len(boxes) + target]) == bytes(ser_one[s])
+
+
+def test_batch_rejects_mixed_kinds(gpu):
+    from yukawamd_b200._lib import EngineError
+    with pytest.raises(EngineError) as ei:
+        Batch([ion_boxes()[0], nucleon_boxes()[0]])
+    assert ei.value.code == abi.YK_ERR_ARG

@@ -7,6 +7,6 @@ reference's accel(do_measurements) / newton(do_measurements) interface.
 """
 from . import abi  # noqa: F401
 from ._lib import EngineError, lib  # noqa: F401
-from .engine import Engine  # noqa: F401
+from .engine import Batch, Engine  # noqa: F401
 
-__all__ = ["abi", "Engine", "EngineError", "lib"]
+__all__ = ["abi", "Batch", "Engine", "EngineError", "lib"]

@@ -31,6 +31,13 @@ SIGNATURES = {
     "yk_get_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_box": (C.c_int, [_ctx, _dp]),
+    "yk_batch_create": (C.c_int, [C.c_int, _P, C.POINTER(C.c_int), C.POINTER(_dp), C.POINTER(_dp),
+                                  C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(_ctx)]),
+    "yk_batch_destroy": (C.c_int, [_ctx]),
+    "yk_batch_last_error": (C.c_char_p, [_ctx]),
+    "yk_batch_accel": (C.c_int, [_ctx, C.c_int, _S]),
+    "yk_batch_run": (C.c_int, [_ctx, C.c_int, C.c_int, _S, C.POINTER(C.c_double)]),
+    "yk_batch_get_state": (C.c_int, [_ctx, C.c_int, _dp, _dp, _dp, _dp]),
     "yk_get_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_set_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_perf_enable": (C.c_int, [_ctx, C.c_int, C.c_size_t]),
@@ -71,4 +78,10 @@ def lib():
 def check(code, ctx=None):
     if code != abi.YK_OK:
         msg = lib().yk_last_error(ctx)
+        raise EngineError(code, msg.decode() if msg else "")
+
+
+def check_batch(code, b=None):
+    if code != abi.YK_OK:
+        msg = lib().yk_batch_last_error(b)
         raise EngineError(code, msg.decode() if msg else "")

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libyukawa_b200.so")
 
-SOURCES = ["yk_engine.cu"]
+SOURCES = ["yk_engine.cu", "yk_batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
          "-cudart", "static", "--expt-relaxed-constexpr",

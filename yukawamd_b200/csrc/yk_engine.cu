@@ -22,6 +22,7 @@
 
 #include "../../include/yukawa_engine.h"
 #include "yk_force.cuh"
+#include "yk_internal.h"
 #include "yk_pairs.cuh"
 #include "yk_sort.cuh"
 #include "yk_verlet.cuh"
@@ -244,6 +245,21 @@ static void setup_args(yk_ctx* c)
     c->nfb = (c->n + FBLOCK - 1) / FBLOCK;
     c->nvb = (c->n + VBLOCK - 1) / VBLOCK;
 }
+
+namespace yk {
+void make_args(const yk_params& p, int n, ForceArgs* fa, StepArgs* sa, FinishArgs* fz)
+{
+    yk_ctx tmp;
+    tmp.p = p;
+    tmp.n = n;
+    setup_args(&tmp);
+    *fa = tmp.fa;
+    *sa = tmp.sa;
+    *fz = tmp.fz_base;
+}
+
+void count_launches(int k) { g_launches += k; }
+}  // namespace yk
 
 static void drop_graphs(yk_ctx* c)
 {

@@ -141,119 +141,160 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
     }
 }
 
+// Shared memory of the half-pair kernels.
+struct PairSmem {
+    double4 tile[2][PB];                  // FP64 source tiles (TMA)
+    float tilef[2][4 * SHADOW_TILE];      // FP32 shadow source tiles (TMA)
+    double acc_j[2][PWARPS][PB * 3];      // per-warp reaction rows, double-buffered by tile
+    double red[32 * NSCAL];               // block reduction scratch
+    uint64_t bar[2];                      // one mbarrier per tile stage
+    int s_job;
+};
+
+// One box as a job sees it: base pointers of its slots, shadow tiles and
+// scratch, and its tile geometry.
+struct BoxView {
+    const double4* pos;
+    const float* posf;
+    double* Si;
+    double* Sj;
+    int n, M, seg, nseg_max;
+};
+
+__device__ __forceinline__ void pairs_smem_init(PairSmem& sm)
+{
+    if (threadIdx.x == 0) {
+        mbar_init(&sm.bar[0], 1);
+        mbar_init(&sm.bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
+
+// Load source tile C of box bx into stage qq & 1 (thread 0 only).
+__device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int C, unsigned qq)
+{
+    const int j0 = C * PB;
+    const int cnt = min(PB, bx.n - j0);
+    const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
+    const unsigned bytesf = 4u * SHADOW_TILE * (unsigned)sizeof(float);
+    uint64_t* b = &sm.bar[qq & 1];
+    mbar_arrive_expect_tx(b, bytes + bytesf);
+    bulk_g2s(&sm.tile[qq & 1][0], bx.pos + j0, bytes, b);
+    bulk_g2s(&sm.tilef[qq & 1][0], bx.posf + (size_t)C * 4 * SHADOW_TILE, bytesf, b);
+}
+
+// Job (R, sg) of box bx: target block R against source tiles
+// C = R + sg*seg ... (at most seg of them).  q counts the tiles this CTA has
+// consumed (stage and mbarrier parity).  Writes Si / Sj rows of the box and,
+// when measuring, the job's 8 sums to sm_row.  Returns false if a tile copy
+// timed out (the CTA must then leave).
+template <int SIM, int PREC, bool MEAS>
+__device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, const BoxView& bx, int R, int sg,
+                                          double* __restrict__ sm_row, unsigned* __restrict__ err,
+                                          unsigned& q)
+{
+    using R_t = real_t<PREC>;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int n = bx.n;
+    const int C0 = R + sg * bx.seg;
+    const int C1 = min(C0 + bx.seg, bx.M);
+    const int i = R * PB + tid;
+    const bool active = i < n;
+    const double4 pi = active ? bx.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const ScreenI si = load_screen_i(bx.posf, active ? i : 0);
+    const R_t wi = (SIM == SIM_MIX) ? (R_t)pi.w : (R_t)1;   // Z_i of the reaction
+    const bool all_active = (R + 1) * PB <= n;
+    TargetAcc<PREC, MEAS> acc;
+    acc.zero();
+
+    if (tid == 0) {
+        pairs_issue(sm, bx, C0, q);
+        if (C0 + 1 < C1) pairs_issue(sm, bx, C0 + 1, q + 1);
+    }
+    for (int C = C0; C < C1; ++C, ++q) {
+        const int st = q & 1;
+        // zero this tile's accumulator rows; the other buffer may still be
+        // read by threads finishing the previous tile's sum
+#pragma unroll
+        for (int w = 0; w < PWARPS; ++w) {
+            sm.acc_j[st][w][3 * tid] = 0.0;
+            sm.acc_j[st][w][3 * tid + 1] = 0.0;
+            sm.acc_j[st][w][3 * tid + 2] = 0.0;
+        }
+        const bool ok = mbar_wait_bounded(&sm.bar[st], (q >> 1) & 1u, err);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0 && C + 1 < C1) mbar_wait_bounded(&sm.bar[st ^ 1], ((q + 1) >> 1) & 1u, err);
+            return false;
+        }
+        const int jlim = min(PB, n - C * PB);
+        const bool diag = (C == R);
+        const double4* tl = sm.tile[st];
+        const float* tlf = sm.tilef[st];
+        double* my_acc = sm.acc_j[st][warp];
+        const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
+        if (!diag && jlim == PB && all_active) {
+            for (int j0 = 0; j0 < PB; j0 += 4)
+                pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active, tid, sw,
+                                                   acc, my_acc);
+        } else {
+            for (int j0 = 0; j0 < jlim; j0 += 4)
+                pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active, tid, sw,
+                                                  acc, my_acc);
+        }
+        __syncthreads();                  // tile done: stage st reusable, rows complete
+        if (tid == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2);
+        // source-side partial of unit (R, C): the warp rows in fixed order
+        double* dj = bx.Sj + ((size_t)tri_index(C, R) * PB + tid) * 3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double v = sm.acc_j[st][0][3 * tid + c];
+#pragma unroll
+            for (int w = 1; w < PWARPS; ++w) v += sm.acc_j[st][w][3 * tid + c];
+            dj[c] = v;
+        }
+    }
+    // target-side partial of job (R, s)
+    double* di = bx.Si + (((size_t)R * bx.nseg_max + sg) * PB + tid) * 3;
+    di[0] = acc.force(0);
+    di[1] = acc.force(1);
+    di[2] = acc.force(2);
+    if constexpr (MEAS) {
+        double S[NSCAL];
+#pragma unroll
+        for (int k = 0; k < NSCAL; ++k) S[k] = active ? acc.scal(k) * (double)wi : 0.0;
+        block_sum_store<NSCAL>(S, sm.red, sm_row);
+        __syncthreads();
+    }
+    return true;
+}
+
 template <int SIM, int PREC, bool MEAS>
 __global__ void __launch_bounds__(PB, 5)
 k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, PairJobs pj,
               int* __restrict__ job_counter, ForceArgs fa, double* __restrict__ Si,
               double* __restrict__ Sj, double* __restrict__ Sm, unsigned* __restrict__ err)
 {
-    __shared__ __align__(128) double4 tile[2][PB];
-    __shared__ __align__(128) float tilef[2][4 * SHADOW_TILE];
-    __shared__ double acc_j[2][PWARPS][PB * 3];    // double-buffered by tile
-    __shared__ double red[32 * NSCAL];
-    __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int s_job;
-
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
-    const int n = fa.n;
-    using R_t = real_t<PREC>;
-
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    unsigned q = 0;               // tiles this CTA has consumed (stage / parity)
-    auto issue = [&](int C, unsigned qq) {
-        const int j0 = C * PB;
-        const int cnt = min(PB, n - j0);
-        const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
-        const unsigned bytesf = 4u * SHADOW_TILE * (unsigned)sizeof(float);
-        uint64_t* b = &bar[qq & 1];
-        mbar_arrive_expect_tx(b, bytes + bytesf);
-        bulk_g2s(&tile[qq & 1][0], pos + j0, bytes, b);
-        bulk_g2s(&tilef[qq & 1][0], posf + (size_t)C * 4 * SHADOW_TILE, bytesf, b);
-    };
-
+    __shared__ __align__(128) PairSmem sm;
+    pairs_smem_init(sm);
+    BoxView bx;
+    bx.pos = pos;
+    bx.posf = posf;
+    bx.Si = Si;
+    bx.Sj = Sj;
+    bx.n = fa.n;
+    bx.M = pj.M;
+    bx.seg = pj.seg;
+    bx.nseg_max = pj.nseg_max;
+    unsigned q = 0;
     for (;;) {
-        if (tid == 0) s_job = atomicAdd(job_counter, 1);
+        if (threadIdx.x == 0) sm.s_job = atomicAdd(job_counter, 1);
         __syncthreads();
-        const int job = s_job;
+        const int job = sm.s_job;
         if (job >= pj.njobs) break;
         const int2 js = pj.jobs[job];
-        const int R = js.x, sg = js.y;
-        const int C0 = R + sg * pj.seg;
-        const int C1 = min(C0 + pj.seg, pj.M);
-        const int i = R * PB + tid;
-        const bool active = i < n;
-        const double4 pi = active ? pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
-        const ScreenI si = load_screen_i(posf, active ? i : 0);
-        const R_t wi = (SIM == SIM_MIX) ? (R_t)pi.w : (R_t)1;   // Z_i of the reaction
-        const bool all_active = (R + 1) * PB <= n;
-        TargetAcc<PREC, MEAS> acc;
-        acc.zero();
-
-        if (tid == 0) {
-            issue(C0, q);
-            if (C0 + 1 < C1) issue(C0 + 1, q + 1);
-        }
-        for (int C = C0; C < C1; ++C, ++q) {
-            const int st = q & 1;
-            // zero this tile's accumulator rows; the other buffer may still
-            // be read by threads finishing the previous tile's sum
-#pragma unroll
-            for (int w = 0; w < PWARPS; ++w) {
-                acc_j[st][w][3 * tid] = 0.0;
-                acc_j[st][w][3 * tid + 1] = 0.0;
-                acc_j[st][w][3 * tid + 2] = 0.0;
-            }
-            const bool ok = mbar_wait_bounded(&bar[st], (q >> 1) & 1u, err);
-            if (__syncthreads_or(!ok)) {
-                if (tid == 0 && C + 1 < C1) mbar_wait_bounded(&bar[st ^ 1], ((q + 1) >> 1) & 1u, err);
-                return;
-            }
-            const int jlim = min(PB, n - C * PB);
-            const bool diag = (C == R);
-            const double4* tl = tile[st];
-            const float* tlf = tilef[st];
-            double* my_acc = acc_j[st][warp];
-            const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
-            if (!diag && jlim == PB && all_active) {
-                for (int j0 = 0; j0 < PB; j0 += 4)
-                    pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active,
-                                                       tid, sw, acc, my_acc);
-            } else {
-                for (int j0 = 0; j0 < jlim; j0 += 4)
-                    pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active,
-                                                      tid, sw, acc, my_acc);
-            }
-            __syncthreads();                  // tile done: stage st reusable, rows complete
-            if (tid == 0 && C + 2 < C1) issue(C + 2, q + 2);
-            // source-side partial of unit (R, C): the warp rows in fixed order
-            double* dj = Sj + ((size_t)tri_index(C, R) * PB + tid) * 3;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                double v = acc_j[st][0][3 * tid + c];
-#pragma unroll
-                for (int w = 1; w < PWARPS; ++w) v += acc_j[st][w][3 * tid + c];
-                dj[c] = v;
-            }
-        }
-        // target-side partial of job (R, s)
-        double* di = Si + (((size_t)R * pj.nseg_max + sg) * PB + tid) * 3;
-        di[0] = acc.force(0);
-        di[1] = acc.force(1);
-        di[2] = acc.force(2);
-        if constexpr (MEAS) {
-            double S[NSCAL];
-#pragma unroll
-            for (int k = 0; k < NSCAL; ++k) S[k] = active ? acc.scal(k) * (double)wi : 0.0;
-            block_sum_store<NSCAL>(S, red, Sm + (size_t)job * NSCAL);
-            __syncthreads();
-        }
+        if (!pairs_job<SIM, PREC, MEAS>(sm, fa, bx, js.x, js.y, Sm + (size_t)job * NSCAL, err, q)) return;
     }
 }
 

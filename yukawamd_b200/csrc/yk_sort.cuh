@@ -25,7 +25,7 @@ __device__ __forceinline__ unsigned spread10(unsigned v)
 }
 
 // keys[i] = Morton code of particle i's cell on a 1024^3 grid over the box.
-__global__ void k_morton(const double* __restrict__ x, int n, double sx, double sy, double sz,
+static __global__ void k_morton(const double* __restrict__ x, int n, double sx, double sy, double sz,
                          unsigned* __restrict__ keys, int* __restrict__ idx)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -38,7 +38,7 @@ __global__ void k_morton(const double* __restrict__ x, int n, double sx, double 
 }
 
 // Slot s holds particle perm[s]; iperm is the inverse; pos is repacked.
-__global__ void k_apply_perm(const int* __restrict__ perm, int* __restrict__ iperm,
+static __global__ void k_apply_perm(const int* __restrict__ perm, int* __restrict__ iperm,
                              const double* __restrict__ x, const double* __restrict__ zii,
                              double4* __restrict__ pos, float* __restrict__ posf, int n,
                              int pack_w)

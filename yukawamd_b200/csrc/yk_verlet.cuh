@@ -58,7 +58,7 @@ __device__ __forceinline__ double drift1(double x, double v, double a, const Ste
 }
 
 // VV2 first half: drift, vold = v, v += dt a.
-__global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold,
+static __global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold,
                             const double* __restrict__ a, const double* __restrict__ zii,
                             const int* __restrict__ iperm, double4* __restrict__ pos,
                             float* __restrict__ posf, StepArgs s)
@@ -79,7 +79,7 @@ __global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, doub
 }
 
 // VV1 first half: drift, v += dt/2 a (vel_verlet_1.f:148-166).
-__global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
+static __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
                             const double* __restrict__ a, const double* __restrict__ zii,
                             const int* __restrict__ iperm, double4* __restrict__ pos,
                             float* __restrict__ posf, StepArgs s)
@@ -100,7 +100,7 @@ __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
 
 // VV3 first half: drift and the first Spreiter-Walter stage
 // (vel_verlet_3.f:255-262; v(2,i) reads the already updated v(1,i)).
-__global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ v,
+static __global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ v,
                             const double* __restrict__ a, const double* __restrict__ zii,
                             const double* __restrict__ aii, const int* __restrict__ iperm,
                             double4* __restrict__ pos, float* __restrict__ posf, StepArgs s)
@@ -182,7 +182,7 @@ k_post_vv2(double* __restrict__ v, const double* __restrict__ vold, double* __re
 }
 
 // VV1 second half: v += dt/2 a; kinetic sums always (vel_verlet_1.f:177-188).
-__global__ void __launch_bounds__(VBLOCK)
+static __global__ void __launch_bounds__(VBLOCK)
 k_post_vv1(double* __restrict__ v, const double* __restrict__ a, const double* __restrict__ aii,
            double* __restrict__ kpart, StepArgs s)
 {
@@ -202,7 +202,7 @@ k_post_vv1(double* __restrict__ v, const double* __restrict__ a, const double* _
 }
 
 // VV3 second half: second Spreiter-Walter stage (vel_verlet_3.f:274-287).
-__global__ void __launch_bounds__(VBLOCK)
+static __global__ void __launch_bounds__(VBLOCK)
 k_post_vv3(double* __restrict__ v, const double* __restrict__ a, const double* __restrict__ zii,
            const double* __restrict__ aii, double* __restrict__ kpart, StepArgs s)
 {
@@ -247,11 +247,11 @@ struct FinishArgs {
 
 // Sums the per-CTA partials in a fixed order, writes the packed raw sums to
 // a(:,n..n+2) (int_ion_pure.f:217-225) and the md_globals scalars
-// (int_ion_pure.f:232-248, vel_verlet_2.f:96-110).  One block of 256.
-__global__ void __launch_bounds__(256)
-k_finish(const double* __restrict__ fpart, const double* __restrict__ kpart, FinishArgs fz,
-         double* __restrict__ a, DevScalars* __restrict__ ds, double* __restrict__ series,
-         int* __restrict__ series_idx)
+// (int_ion_pure.f:232-248, vel_verlet_2.f:96-110).  Called by one block of
+// 256 threads; `series` (13 doubles) may be null.
+__device__ __forceinline__ void finish_body(const double* __restrict__ fpart, const double* __restrict__ kpart,
+                                            const FinishArgs& fz, double* __restrict__ a,
+                                            DevScalars* __restrict__ ds, double* __restrict__ series)
 {
     __shared__ double red[32 * 8];
     __shared__ double tot[8 + NKIN];
@@ -330,16 +330,25 @@ k_finish(const double* __restrict__ fpart, const double* __restrict__ kpart, Fin
     }
     *ds = s;
     if (series) {
-        const int idx = *series_idx;
-        double* o = series + (size_t)idx * 13;
-        o[0] = s.ev;
-        o[1] = s.vir;
-        o[2] = s.px;
-        o[3] = s.ek;
+        series[0] = s.ev;
+        series[1] = s.vir;
+        series[2] = s.px;
+        series[3] = s.ek;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) o[4 + k] = s.pp[k];
-        *series_idx = idx + 1;
+        for (int k = 0; k < 9; ++k) series[4 + k] = s.pp[k];
     }
+}
+
+// Single box: one block of 256; the series slot is taken from *series_idx.
+static __global__ void __launch_bounds__(256)
+k_finish(const double* __restrict__ fpart, const double* __restrict__ kpart, FinishArgs fz,
+         double* __restrict__ a, DevScalars* __restrict__ ds, double* __restrict__ series,
+         int* __restrict__ series_idx)
+{
+    double* slot = nullptr;
+    if (series) slot = series + (size_t)(*series_idx) * 13;
+    finish_body(fpart, kpart, fz, a, ds, slot);
+    if (series && threadIdx.x == 0) *series_idx += 1;
 }
 
 }  // namespace yk

@@ -16,7 +16,7 @@ import ctypes as C
 import numpy as np
 
 from . import abi
-from ._lib import check, lib
+from ._lib import check, check_batch, lib
 
 _dp = C.POINTER(C.c_double)
 
@@ -147,6 +147,79 @@ class Engine:
         if self._ctx:
             self._lib.yk_destroy(self._ctx)
             self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent boxes advanced together (one persistent force kernel
+    over all boxes' work items, CUDA graphs of K steps).  boxes: a list of
+    configs.Workload, or of (YkParams, x, v, zii, aii) tuples."""
+
+    def __init__(self, boxes, device=0, **overrides):
+        params, xs, vs, zs, ms = [], [], [], [], []
+        for b in boxes:
+            if isinstance(b, tuple):
+                p, x, v, z, m = b
+            else:
+                p = b.yk_params(**overrides)
+                x, v, z, m = b.x, b.v, b.zii, b.aii
+            params.append(p)
+            xs.append(_f64(x))
+            vs.append(_f64(v))
+            zs.append(_f64(z))
+            ms.append(_f64(m))
+        self.nrep = len(params)
+        self.n = [len(x) // 3 for x in xs]
+        self._keep = (xs, vs, zs, ms)
+        P = (abi.YkParams * self.nrep)(*params)
+        self.params = P
+        N = (C.c_int * self.nrep)(*self.n)
+
+        def ptrs(arrs):
+            return (_dp * self.nrep)(*[_ptr(a) if a is not None else None for a in arrs])
+        self._lib = lib()
+        self._b = C.c_void_p()
+        check_batch(self._lib.yk_batch_create(self.nrep, P, N, ptrs(xs), ptrs(vs), ptrs(zs), ptrs(ms),
+                                              int(device), C.byref(self._b)))
+        self._keep = None
+
+    def accel(self, do_measurements=True):
+        out = (abi.YkScalars * self.nrep)()
+        check_batch(self._lib.yk_batch_accel(self._b, int(bool(do_measurements)), out), self._b)
+        return out
+
+    def run(self, nsteps, meas_every=0, series=True):
+        """Returns (series or None, milliseconds of device time); series is a
+        ctypes array indexed [step * nrep + box]."""
+        buf = (abi.YkScalars * (nsteps * self.nrep))() if series and nsteps > 0 else None
+        ms = C.c_double()
+        check_batch(self._lib.yk_batch_run(self._b, int(nsteps), int(meas_every), buf, C.byref(ms)),
+                    self._b)
+        return buf, ms.value
+
+    def get_state(self, rep):
+        n = self.n[rep]
+        x, v, vold = (np.empty(3 * n) for _ in range(3))
+        a = np.empty(3 * (n + 3))
+        check_batch(self._lib.yk_batch_get_state(self._b, int(rep), _ptr(x), _ptr(v), _ptr(vold),
+                                                 _ptr(a)), self._b)
+        return x, v, vold, a
+
+    def close(self):
+        if self._b:
+            self._lib.yk_batch_destroy(self._b)
+            self._b = C.c_void_p()
 
     def __enter__(self):
         return self

@@ -1,0 +1,120 @@
+"""Autotuner for the engine's tunables.
+
+For one box the engine can run its force call two ways (the half-pair kernel
+with scratch, or the row kernel that evaluates each pair from both sides)
+and cut the half-pair work into jobs of `pair_seg` source tiles; it refreshes
+the Morton order every `sort_every` steps.  Which choice is fastest depends on
+N, the cutoff radius relative to the box, the interaction and the precision,
+so the tuner measures candidates on the caller's own workload (CUDA-event
+time of the force call, yk_perf) and remembers the winner per
+
+    (GPU name, sim type, precision, N bucket)      N bucket = round(2 log2 N)
+
+in a JSON cache (default ~/.cache/yukawamd_b200/tune.json, or $YK_TUNE_CACHE).
+Engine.autotune() / tune.apply(engine) use it transparently.
+"""
+import json
+import math
+import os
+import time
+
+from . import abi
+
+CANDIDATES = [
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=50),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=4, sort_every=50),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=16, sort_every=50),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=2, sort_every=50),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=20),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=-1),
+    dict(force_kernel=abi.KERNEL_ROWS, pair_seg=8, sort_every=50),
+]
+
+
+def cache_path():
+    p = os.environ.get("YK_TUNE_CACHE")
+    if p:
+        return p
+    base = os.environ.get("XDG_CACHE_HOME", os.path.join(os.path.expanduser("~"), ".cache"))
+    return os.path.join(base, "yukawamd_b200", "tune.json")
+
+
+def _load():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(doc):
+    path = cache_path()
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + ".tmp%d" % os.getpid()
+    with open(tmp, "w") as f:
+        json.dump(doc, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def gpu_name(device=0):
+    try:
+        import torch
+        return torch.cuda.get_device_name(device)
+    except Exception:
+        return "cuda:%d" % device
+
+
+def bucket(n):
+    return int(round(2.0 * math.log2(max(n, 1))))
+
+
+def key_for(engine, device=0):
+    p = engine.params
+    return "%s|sim%d|prec%d|nb%d" % (gpu_name(device), p.sim_type, p.precision, bucket(engine.n))
+
+
+def measure(engine, cand, steps=6, warmup=2):
+    """Mean CUDA-event time (ms) of the force call under candidate `cand`.
+    The engine's state advances by warmup + steps steps."""
+    engine.set_tuning(**cand)
+    engine.run(warmup, 0, series=False)
+    engine.perf_enable(True, 0)
+    engine.run(steps, 0, series=False)
+    perf = engine.perf_read()
+    engine.perf_enable(False, 0)
+    return perf.force_ms / max(perf.force_calls, 1)
+
+
+def tune(engine, candidates=None, steps=6, warmup=2, device=0, save=True):
+    """Time every candidate on this engine's workload; apply and return the
+    best one.  The engine's positions are restored afterwards, so tuning does
+    not advance the caller's trajectory."""
+    candidates = candidates or CANDIDATES
+    x, v, vold, a = engine.get_state()
+    results = []
+    for cand in candidates:
+        try:
+            ms = measure(engine, cand, steps, warmup)
+        except Exception as exc:          # e.g. scratch too large for this N
+            results.append((float("inf"), cand, str(exc)))
+            continue
+        results.append((ms, cand, None))
+        engine.set_state(x=x, v=v, vold=vold, a=a)
+    best_ms, best, _ = min(results, key=lambda r: r[0])
+    engine.set_tuning(**best)
+    engine.set_state(x=x, v=v, vold=vold, a=a)
+    if save:
+        doc = _load()
+        doc[key_for(engine, device)] = dict(best, force_ms=best_ms, when=time.time(),
+                                            n=engine.n, tried=[(r[0], r[1]) for r in results])
+        _store(doc)
+    return best, best_ms, results
+
+
+def apply(engine, device=0):
+    """Apply the cached choice for this engine's bucket; True if one existed."""
+    ent = _load().get(key_for(engine, device))
+    if not ent:
+        return False
+    engine.set_tuning(**{k: ent[k] for k in ("force_kernel", "pair_seg", "sort_every") if k in ent})
+    return True
