@@ -63,6 +63,18 @@ def parse():
                     help="skip the mixed-precision companion measurement")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the nucleon and replica-ensemble side measurements")
+    ap.add_argument("--drift", type=int, default=0,
+                    help="instead of the benchmark: run this many steps in FP64 and in mixed "
+                         "precision and report the total-energy drift")
+    ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--serve", action="store_true",
+                    help="instead of the benchmark: serve a request stream and report latency")
+    ap.add_argument("--serve-count", type=int, default=48)
+    ap.add_argument("--serve-rate", type=float, default=8.0)
+    ap.add_argument("--serve-nmax", type=int, default=32768)
+    ap.add_argument("--serve-smax", type=int, default=1000)
     return ap.parse_args()
 
 
@@ -378,6 +390,10 @@ def run_ours(args, dist):
                       "px_rel_err": px_err}
         e2.close()
 
+    if not args.no_extras and dist.world == 1:
+        out["nucleon"] = nucleon_pair(K, W, me, dist)
+        out["ensemble"] = ensemble(args.ensemble_steps, me, dist)
+
     if not args.no_e2e:
         t_e2e, bi, bo = e2e_engine(w, K, W, me, dist)
         t_e2e = dist.max(t_e2e)
@@ -390,6 +406,93 @@ def run_ours(args, dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_sample(w, kind)
     return out
+
+
+def nucleon_pair(K, W, me, dist):
+    """int_nn.f at N = 51,200 (proton fraction 0.4, n_B = 0.05 fm^-3, kT = 1
+    MeV): FP64 and mixed pairs/s and the mixed form's accuracy."""
+    from yukawamd_b200 import abi
+    from yukawamd_b200.engine import Engine
+    w = make_workload("nucleon", 3 + dist.rank)
+    res = {"workload": workload_desc(w, "nucleon"), "pairs_per_step": w.pairs_per_step}
+    for prec in ("fp64", "mixed"):
+        e, perf, _ = time_engine(w, prec, K, W, me, dist)
+        res[prec] = {"value": w.pairs_per_step * K / (dist.max(perf.run_ms) * 1e-3),
+                     "ms_per_step": perf.run_ms / K}
+        e.close()
+    res["ratio_mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    with Engine(w, device=dist.local) as a64, \
+            Engine(w, device=dist.local, precision=abi.YK_PREC_MIXED) as a32:
+        s64 = a64.accel(True)
+        s32 = a32.accel(True)
+        n = w.n
+        res["force_rms_rel_err_vs_fp64"] = float(np.linalg.norm(a32.a[:3 * n] - a64.a[:3 * n]) /
+                                                 np.linalg.norm(a64.a[:3 * n]))
+        res["ev_rel_err"] = abs(s32.ev - s64.ev) / abs(s64.ev)
+    return res
+
+
+def ensemble(steps, me, dist, precision="mixed", seed=4):
+    """The replica ensemble: 256 pure-ion boxes, N log-uniform in
+    [1e3, 2e4], Gamma U[50,250], kappa U[0.5,2], Z in {6,8,26}, advanced
+    together by the batch engine (CUDA graphs of 50 steps)."""
+    from yukawamd_b200 import abi, configs
+    from yukawamd_b200.engine import Batch
+    boxes = configs.replica_ensemble(seed + 1000 * dist.rank)
+    prec = abi.YK_PREC_MIXED if precision == "mixed" else abi.YK_PREC_FP64
+    pairs = sum(w.pairs_per_step for w in boxes)
+    with Batch(boxes, device=dist.local, precision=prec) as b:
+        b.accel(True)
+        b.run(50, me, series=False)                 # warm-up (one graph)
+        dist.barrier()
+        _, ms = b.run(steps, me, series=False)
+        dist.barrier()
+    ms = dist.max(ms)
+    return {"workload": "%d pure-ion boxes, N log-uniform in [1000, 20000] (sum %d), Gamma U[50,250], "
+                        "kappa U[0.5,2], Z in {6,8,26}; seed %d" % (len(boxes), sum(w.n for w in boxes), seed),
+            "precision": precision, "steps": steps, "graph_steps": 50,
+            "pairs_per_step": pairs, "value": dist.world * pairs * steps / (ms * 1e-3),
+            "ms_per_step": ms / steps}
+
+
+def drift(args, dist):
+    """Total energy E = ev + ek (per particle) every 100 steps over args.drift
+    steps, FP64 and mixed, from the same initial state; reports max |dE/E|."""
+    from yukawamd_b200 import abi
+    from yukawamd_b200.engine import Engine
+    w = make_workload(args.workload, args.seed, args.n)
+    out = {"workload": workload_desc(w, args.workload), "steps": args.drift, "every": 100}
+    for prec in ("fp64", "mixed"):
+        with Engine(w, device=dist.local,
+                    precision=abi.YK_PREC_MIXED if prec == "mixed" else abi.YK_PREC_FP64) as e:
+            s0 = e.accel(True)
+            ek0 = float(np.sum(w.aii * (w.v.reshape(-1, 3) ** 2).sum(1)) * 0.5 * 931.0 / w.n)
+            e0 = s0.ev + ek0
+            t0 = time.perf_counter()
+            ser = e.run(args.drift, 100)
+            wall = time.perf_counter() - t0
+            es = np.array([ser[k].ev + ser[k].ek for k in range(99, args.drift, 100)])
+        out[prec] = {"E0": e0, "E_end": float(es[-1]), "max_abs_dE_over_E": float(np.max(np.abs(es - e0)) / abs(e0)),
+                     "end_dE_over_E": float((es[-1] - e0) / abs(e0)), "wall_s": wall}
+    return out
+
+
+def serve_stream(args, dist):
+    """The served request stream: Poisson arrivals, 70 % ion (pure or mixture)
+    and 30 % nucleon runs, N log-uniform in [512, nmax], steps uniform in
+    [100, smax], mixed precision with an FP64 twin for 1 run in 16."""
+    from yukawamd_b200 import configs
+    from yukawamd_b200.serve import Server, make_requests
+    stream = configs.request_stream(seed=args.seed, count=args.serve_count, rate_per_s=args.serve_rate,
+                                    nmin=512, nmax=args.serve_nmax, smin=100, smax=args.serve_smax)
+    reqs = make_requests(stream, shadow_every=16)
+    srv = Server(device=dist.local, chunk=50)
+    rep = srv.run(reqs)
+    rep.update({"metric": "served p99 completion latency; aggregate pair-interactions/s",
+                "stream": "%d runs, Poisson rate %.2f/s, 70%% ion / 30%% nucleon, N log-uniform in "
+                          "[512, %d], steps U[100, %d], mixed precision, FP64 twin 1 in 16, seed %d"
+                          % (args.serve_count, args.serve_rate, args.serve_nmax, args.serve_smax, args.seed)})
+    return rep
 
 
 def run_reference(args):
@@ -450,6 +553,16 @@ def main():
     dist = Dist()
     dist.init()
     try:
+        if args.serve:
+            out = serve_stream(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(out), flush=True)
+            return 0
+        if args.drift:
+            out = drift(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(out), flush=True)
+            return 0
         out = run_ours(args, dist)
         if dist.rank == 0:
             print(json.dumps(out), flush=True)

@@ -200,9 +200,13 @@ YK_API int yk_batch_accel(yk_batch* b, int do_meas, yk_scalars* out);
  * device work or NULL. */
 YK_API int yk_batch_run(yk_batch* b, int nsteps, int meas_every,
                         yk_scalars* series, double* ms);
-/* State of box rep: x, v, vold double[3 n[rep]]; a double[3(n[rep]+3)]. */
+/* State of box rep: x, v, vold double[3 n[rep]]; a double[3(n[rep]+3)].
+ * Any pointer may be NULL. */
 YK_API int yk_batch_get_state(yk_batch* b, int rep, double* x, double* v,
                               double* vold, double* a);
+YK_API int yk_batch_set_state(yk_batch* b, int rep, const double* x,
+                              const double* v, const double* vold,
+                              const double* a);
 
 /*
  * Engine tunables (not reference parameters): which force kernel runs and

@@ -38,6 +38,7 @@ SIGNATURES = {
     "yk_batch_accel": (C.c_int, [_ctx, C.c_int, _S]),
     "yk_batch_run": (C.c_int, [_ctx, C.c_int, C.c_int, _S, C.POINTER(C.c_double)]),
     "yk_batch_get_state": (C.c_int, [_ctx, C.c_int, _dp, _dp, _dp, _dp]),
+    "yk_batch_set_state": (C.c_int, [_ctx, C.c_int, _dp, _dp, _dp, _dp]),
     "yk_get_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_set_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_perf_enable": (C.c_int, [_ctx, C.c_int, C.c_size_t]),

@@ -806,4 +806,26 @@ int yk_batch_get_state(yk_batch* b, int rep, double* x, double* v, double* vold,
     return YK_OK;
 }
 
+int yk_batch_set_state(yk_batch* b, int rep, const double* x, const double* v, const double* vold,
+                       const double* a)
+{
+    if (!b) return bfail(nullptr, YK_ERR_ARG, "batch is NULL");
+    if (rep < 0 || rep >= b->nrep) return bfail(b, YK_ERR_ARG, "box %d out of range", rep);
+    const size_t cnt = 3 * (size_t)b->n[rep];
+    for (size_t e = 0; e < cnt; ++e)
+        if ((x && !std::isfinite(x[e])) || (v && !std::isfinite(v[e])) || (vold && !std::isfinite(vold[e])))
+            return bfail(b, YK_ERR_NONFINITE, "box %d: NaN or Inf in a state array", rep);
+    BCK(b, cudaSetDevice(b->dev));
+    const size_t off = 3 * (size_t)b->P[rep], bytes = sizeof(double) * cnt;
+    cudaStream_t st = b->stream;
+    if (x) BCK(b, cudaMemcpyAsync(b->x + off, x, bytes, cudaMemcpyHostToDevice, st));
+    if (v) BCK(b, cudaMemcpyAsync(b->v + off, v, bytes, cudaMemcpyHostToDevice, st));
+    if (vold) BCK(b, cudaMemcpyAsync(b->vold + off, vold, bytes, cudaMemcpyHostToDevice, st));
+    if (a) BCK(b, cudaMemcpyAsync(b->a + b->A[rep], a, sizeof(double) * 3 * (size_t)(b->n[rep] + 3),
+                                  cudaMemcpyHostToDevice, st));
+    if (x) b->pos_dirty = true;
+    BCK(b, cudaStreamSynchronize(st));
+    return YK_OK;
+}
+
 }  // extern "C"

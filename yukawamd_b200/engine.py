@@ -216,6 +216,11 @@ class Batch:
                                                  _ptr(a)), self._b)
         return x, v, vold, a
 
+    def set_state(self, rep, x=None, v=None, vold=None, a=None):
+        x, v, vold, a = _f64(x), _f64(v), _f64(vold), _f64(a)
+        check_batch(self._lib.yk_batch_set_state(self._b, int(rep), _ptr(x), _ptr(v), _ptr(vold),
+                                                 _ptr(a)), self._b)
+
     def close(self):
         if self._b:
             self._lib.yk_batch_destroy(self._b)
