@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--drift", type=int, default=0,
                     help="instead of the benchmark: run this many steps in FP64 and in mixed "
                          "precision and report the total-energy drift")
+    ap.add_argument("--drift-warmup", type=int, default=20,
+                    help="warm-up groups of 100 steps (cancel_vcom + tnorm after each) before --drift")
     ap.add_argument("--ensemble-steps", type=int, default=100)
     ap.add_argument("--serve", action="store_true",
                     help="instead of the benchmark: serve a request stream and report latency")
@@ -457,17 +459,29 @@ def ensemble(steps, me, dist, precision="mixed", seed=4):
 
 def drift(args, dist):
     """Total energy E = ev + ek (per particle) every 100 steps over args.drift
-    steps, FP64 and mixed, from the same initial state; reports max |dE/E|."""
+    steps, FP64 and mixed, from the same equilibrated state; reports max |dE/E|.
+    The state comes from the reference's warm-up (md.F:87-101): args.drift_warmup
+    groups of 100 FP64 steps, each followed by cancel_vcom and tnorm, all on the
+    device through the run driver."""
     from yukawamd_b200 import abi
+    from yukawamd_b200.driver import RunControl, run_md
     from yukawamd_b200.engine import Engine
     w = make_workload(args.workload, args.seed, args.n)
-    out = {"workload": workload_desc(w, args.workload), "steps": args.drift, "every": 100}
+    out = {"workload": workload_desc(w, args.workload), "steps": args.drift, "every": 100,
+           "warmup": "%d groups x 100 FP64 steps with cancel_vcom + tnorm (md.F:87-101)" % args.drift_warmup}
+    x, v = w.x, w.v
+    if args.drift_warmup > 0:
+        with Engine(w, device=dist.local, precision=abi.YK_PREC_FP64) as e:
+            t0 = time.perf_counter()
+            res = run_md(e, RunControl(nwgroup=args.drift_warmup, nwsteps=100))
+            out["warmup_wall_s"] = time.perf_counter() - t0
+            out["E_initial_raw"] = res.initial["e"]
+            x, v, _vold, _a = e.get_state()
     for prec in ("fp64", "mixed"):
-        with Engine(w, device=dist.local,
-                    precision=abi.YK_PREC_MIXED if prec == "mixed" else abi.YK_PREC_FP64) as e:
+        yp = w.yk_params(precision=abi.YK_PREC_MIXED if prec == "mixed" else abi.YK_PREC_FP64)
+        with Engine(yp, x, v, w.zii, w.aii, device=dist.local) as e:
             s0 = e.accel(True)
-            ek0 = float(np.sum(w.aii * (w.v.reshape(-1, 3) ** 2).sum(1)) * 0.5 * 931.0 / w.n)
-            e0 = s0.ev + ek0
+            e0 = s0.ev + e.ttot()
             t0 = time.perf_counter()
             ser = e.run(args.drift, 100)
             wall = time.perf_counter() - t0

@@ -166,6 +166,21 @@ YK_API int yk_get_state(yk_ctx* ctx, double* x, double* v, double* vold, double*
 YK_API int yk_set_state(yk_ctx* ctx, const double* x, const double* v,
                  const double* vold, const double* a);
 
+/* The reference driver's per-step host passes, on the device state
+ * (gen_utils.f:40-110, strain.f:19-82):
+ *   yk_ttot         average kinetic energy per particle -> *eka
+ *   yk_tnorm        rescale velocities to eka = 1.5 kT
+ *   yk_cancel_vcom  remove the centre-of-mass velocity, then tnorm
+ *   yk_strain       volume-preserving normal strain of the box at rates
+ *                   deps (1000 = no strain in that direction) relative to
+ *                   the gage dimensions xl0, then re-wrap x > xl; the new
+ *                   edge lengths go to xl_out (may be NULL). */
+YK_API int yk_ttot(yk_ctx* ctx, double* eka);
+YK_API int yk_tnorm(yk_ctx* ctx);
+YK_API int yk_cancel_vcom(yk_ctx* ctx);
+YK_API int yk_strain(yk_ctx* ctx, const double deps[3], const double xl0[3],
+                     double xl_out[3]);
+
 /* New box edge lengths (strain.f changes xl every step). */
 YK_API int yk_set_box(yk_ctx* ctx, const double xl[3]);
 

@@ -31,6 +31,10 @@ SIGNATURES = {
     "yk_get_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_box": (C.c_int, [_ctx, _dp]),
+    "yk_ttot": (C.c_int, [_ctx, _dp]),
+    "yk_tnorm": (C.c_int, [_ctx]),
+    "yk_cancel_vcom": (C.c_int, [_ctx]),
+    "yk_strain": (C.c_int, [_ctx, _dp, _dp, _dp]),
     "yk_batch_create": (C.c_int, [C.c_int, _P, C.POINTER(C.c_int), C.POINTER(_dp), C.POINTER(_dp),
                                   C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(_ctx)]),
     "yk_batch_destroy": (C.c_int, [_ctx]),

@@ -25,6 +25,7 @@
 #include "yk_internal.h"
 #include "yk_pairs.cuh"
 #include "yk_sort.cuh"
+#include "yk_thermo.cuh"
 #include "yk_verlet.cuh"
 
 using namespace yk;
@@ -84,6 +85,7 @@ struct yk_ctx {
     size_t cub_bytes = 0;
     // reductions and outputs
     double *fpart = nullptr, *kpart = nullptr;
+    double *vpart = nullptr, *vsums = nullptr;   // ttot / tnorm / cancel_vcom sums
     DevScalars* ds = nullptr;
     unsigned* err = nullptr;
     double* series = nullptr;
@@ -682,7 +684,8 @@ int yk_destroy(yk_ctx* c)
     drop_graphs(c);
     free_pairs(c);
     void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->posf, c->perm, c->iperm,
-                    c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->ds, c->err,
+                    c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->vpart, c->vsums,
+                    c->ds, c->err,
                     c->series, c->series_idx, c->job_counter, c->flush_buf};
     for (void* b : bufs) cudaFree(b);
     cudaFreeHost(c->h_ds);
@@ -772,6 +775,8 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     ALLOC(c->idx0, n);
     ALLOC(c->fpart, 8 * (size_t)c->nfb);
     ALLOC(c->kpart, NKIN * (size_t)c->nvb);
+    ALLOC(c->vpart, NVSUM * (size_t)c->nvb);
+    ALLOC(c->vsums, 8);
     ALLOC(c->ds, 1);
     ALLOC(c->err, 1);
     ALLOC(c->series_idx, 1);
@@ -1016,6 +1021,121 @@ int yk_set_box(yk_ctx* c, const double xl[3])
     setup_args(c);
     drop_graphs(c);
     return YK_OK;
+}
+
+// ---- gen_utils.f / strain.f on the device ---------------------------------
+
+static_assert(TBLOCK == VBLOCK, "k_vsums runs on the Verlet block count nvb");
+
+static int enqueue_vsums(yk_ctx* c)
+{
+    k_vsums<<<c->nvb, TBLOCK, 0, c->stream>>>(c->v, c->aii, c->n, c->vpart);
+    k_vreduce<<<1, TBLOCK, 0, c->stream>>>(c->vpart, c->nvb, c->vsums);
+    return 2;
+}
+
+static int enqueue_tnorm(yk_ctx* c)
+{
+    int k = enqueue_vsums(c);
+    k_vscale<<<(3 * c->n + 255) / 256, 256, 0, c->stream>>>(c->v, c->n, c->vsums, c->p.xmass,
+                                                           (double)(float)c->n, c->p.kT);
+    return k + 1;
+}
+
+int yk_ttot(yk_ctx* c, double* eka)
+{
+    if (!c || !eka) return fail(c, YK_ERR_ARG, "ctx and eka are required");
+    CK(c, cudaSetDevice(c->dev));
+    g_launches += enqueue_vsums(c);
+    double h[NVSUM];
+    CK(c, cudaMemcpyAsync(h, c->vsums, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    *eka = (0.5 * c->p.xmass * h[4]) / (double)(float)c->n;     // gen_utils.f:52
+    return YK_OK;
+}
+
+int yk_tnorm(yk_ctx* c)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    if (!(c->p.kT > 0.0)) return fail(c, YK_ERR_ARG, "tnorm needs kT > 0");
+    CK(c, cudaSetDevice(c->dev));
+    g_launches += enqueue_tnorm(c);
+    return sync_and_check(c);
+}
+
+int yk_cancel_vcom(yk_ctx* c)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    if (!(c->p.kT > 0.0)) return fail(c, YK_ERR_ARG, "cancel_vcom ends with tnorm, which needs kT > 0");
+    CK(c, cudaSetDevice(c->dev));
+    int k = enqueue_vsums(c);
+    k_vshift<<<(3 * c->n + 255) / 256, 256, 0, c->stream>>>(c->v, c->n, c->vsums);
+    k += 1 + enqueue_tnorm(c);
+    g_launches += k;
+    return sync_and_check(c);
+}
+
+int yk_strain(yk_ctx* c, const double deps[3], const double xl0[3], double xl_out[3])
+{
+    if (!c || !deps || !xl0) return fail(c, YK_ERR_ARG, "ctx, deps and xl0 are required");
+    CK(c, cudaSetDevice(c->dev));
+    // strain.f:31-69: new edge lengths (volume-preserving normal strain)
+    const double XNOSTRAIN = 1000.0, dt = c->p.dt;
+    double xl[3] = {c->p.xl[0], c->p.xl[1], c->p.xl[2]};
+    const int sel = (deps[0] != XNOSTRAIN ? 1 : 0) + (deps[1] != XNOSTRAIN ? 2 : 0) + (deps[2] != XNOSTRAIN ? 4 : 0);
+    switch (sel) {
+    case 0: break;
+    case 1:
+        xl[0] = xl[0] + deps[0] * dt * xl0[0];
+        xl[1] = xl0[1] * std::sqrt(xl0[0] / xl[0]);
+        xl[2] = xl0[2] * std::sqrt(xl0[0] / xl[0]);
+        break;
+    case 2:
+        xl[1] = xl[1] + deps[1] * dt * xl0[1];
+        xl[0] = xl0[0] * std::sqrt(xl0[1] / xl[1]);
+        xl[2] = xl0[2] * std::sqrt(xl0[1] / xl[1]);
+        break;
+    case 3:
+        xl[0] = xl[0] + deps[0] * dt * xl0[0];
+        xl[1] = xl[1] + deps[1] * dt * xl0[1];
+        xl[2] = xl0[2] * (xl0[0] / xl[0]) * (xl0[1] / xl[1]);
+        break;
+    case 4:
+        xl[2] = xl[2] + deps[2] * dt * xl0[2];
+        xl[0] = xl0[0] * std::sqrt(xl0[2] / xl[2]);
+        xl[1] = xl0[1] * std::sqrt(xl0[2] / xl[2]);
+        break;
+    case 5:
+        xl[0] = xl[0] + deps[0] * dt * xl0[0];
+        xl[2] = xl[2] + deps[2] * dt * xl0[2];
+        xl[1] = xl0[1] * (xl0[0] / xl[0]) * (xl0[2] / xl[2]);
+        break;
+    case 6:
+        xl[1] = xl[1] + deps[1] * dt * xl0[1];
+        xl[2] = xl[2] + deps[2] * dt * xl0[2];
+        xl[0] = xl0[0] * (xl0[1] / xl[1]) * (xl0[2] / xl[2]);
+        break;
+    default:
+        xl[0] = xl[0] + deps[0] * dt * xl0[0];
+        xl[1] = xl[1] + deps[1] * dt * xl0[1];
+        xl[2] = xl[2] + deps[2] * dt * xl0[2];
+        break;
+    }
+    for (int k = 0; k < 3; ++k)
+        if (!(xl[k] > 0.0) || !std::isfinite(xl[k])) return fail(c, YK_ERR_ARG, "strain made xl(%d) <= 0", k + 1);
+    // strain.f:73-79 (the re-wrap) runs even without strain
+    k_strain_wrap<<<(3 * c->n + 255) / 256, 256, 0, c->stream>>>(c->x, c->n, xl[0], xl[1], xl[2]);
+    g_launches += 1;
+    if (sel != 0) {
+        for (int k = 0; k < 3; ++k) c->p.xl[k] = xl[k];
+        setup_args(c);
+        drop_graphs(c);
+    }
+    c->pos_dirty = true;
+    if (xl_out)
+        for (int k = 0; k < 3; ++k) xl_out[k] = xl[k];
+    return sync_and_check(c);
 }
 
 int yk_perf_enable(yk_ctx* c, int enable, size_t flush_bytes)

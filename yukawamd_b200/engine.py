@@ -114,6 +114,27 @@ class Engine:
         for k in range(3):
             self.params.xl[k] = float(xl[k])
 
+    # -- gen_utils.f / strain.f on the device ------------------------------
+    def ttot(self):
+        out = C.c_double()
+        check(self._lib.yk_ttot(self._ctx, C.byref(out)), self._ctx)
+        return out.value
+
+    def tnorm(self):
+        check(self._lib.yk_tnorm(self._ctx), self._ctx)
+
+    def cancel_vcom(self):
+        check(self._lib.yk_cancel_vcom(self._ctx), self._ctx)
+
+    def strain(self, deps, xl0):
+        d = (C.c_double * 3)(*[float(t) for t in deps])
+        g = (C.c_double * 3)(*[float(t) for t in xl0])
+        out = (C.c_double * 3)()
+        check(self._lib.yk_strain(self._ctx, C.cast(d, _dp), C.cast(g, _dp), C.cast(out, _dp)), self._ctx)
+        for k in range(3):
+            self.params.xl[k] = out[k]
+        return list(out)
+
     # -- engine tunables (force kernel, job size, sort cadence, graph length) -
     def tuning(self):
         t = abi.YkTuning()
