@@ -166,6 +166,19 @@ YK_API int yk_get_state(yk_ctx* ctx, double* x, double* v, double* vold, double*
 YK_API int yk_set_state(yk_ctx* ctx, const double* x, const double* v,
                  const double* vold, const double* a);
 
+/* Asynchronous state snapshot for checkpoint and save_config
+ * (md_utils.f:19-114, which write x and v, or x, v and a, through
+ * rw_xvb.f:148-203).  yk_snapshot_begin copies the current x, v and a
+ * (any pointer may be NULL; a is double[3*n]) into a device buffer on the
+ * engine's stream, then into the caller's host buffers on a second stream,
+ * and returns without waiting: the following steps run while the copy to
+ * the host drains.  The host buffers hold the snapshot once
+ * yk_snapshot_wait returns; they should be page-locked (yk_host_register)
+ * for the copy to overlap.  A second yk_snapshot_begin first waits for the
+ * one in flight.  The first call allocates the 72*n-byte device buffer. */
+YK_API int yk_snapshot_begin(yk_ctx* ctx, double* x, double* v, double* a);
+YK_API int yk_snapshot_wait(yk_ctx* ctx);
+
 /* The reference driver's per-step host passes, on the device state
  * (gen_utils.f:40-110, strain.f:19-82):
  *   yk_ttot         average kinetic energy per particle -> *eka

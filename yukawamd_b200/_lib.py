@@ -31,6 +31,8 @@ SIGNATURES = {
     "yk_get_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_state": (C.c_int, [_ctx, _dp, _dp, _dp, _dp]),
     "yk_set_box": (C.c_int, [_ctx, _dp]),
+    "yk_snapshot_begin": (C.c_int, [_ctx, _dp, _dp, _dp]),
+    "yk_snapshot_wait": (C.c_int, [_ctx]),
     "yk_ttot": (C.c_int, [_ctx, _dp]),
     "yk_tnorm": (C.c_int, [_ctx]),
     "yk_cancel_vcom": (C.c_int, [_ctx]),

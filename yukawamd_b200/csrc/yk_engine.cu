@@ -119,6 +119,11 @@ struct yk_ctx {
     std::vector<cudaEvent_t> ev_pool;
     int ev_used = 0;
     yk_perf perf{};
+    // asynchronous state snapshots (checkpoint / save_config)
+    double* snap = nullptr;          // 9n doubles: x, v, a
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
+    bool snap_pending = false;
     // cached K-step graphs
     std::vector<GraphEntry> graphs;
     unsigned long long graph_clock = 0;
@@ -681,13 +686,17 @@ int yk_destroy(yk_ctx* c)
     if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->snap_stream) cudaStreamSynchronize(c->snap_stream);
     drop_graphs(c);
     free_pairs(c);
     void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->posf, c->perm, c->iperm,
                     c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->vpart, c->vsums,
                     c->ds, c->err,
-                    c->series, c->series_idx, c->job_counter, c->flush_buf};
+                    c->series, c->series_idx, c->job_counter, c->flush_buf, c->snap};
     for (void* b : bufs) cudaFree(b);
+    if (c->snap_taken) cudaEventDestroy(c->snap_taken);
+    if (c->snap_done) cudaEventDestroy(c->snap_done);
+    if (c->snap_stream) cudaStreamDestroy(c->snap_stream);
     cudaFreeHost(c->h_ds);
     cudaFreeHost(c->h_err);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -984,6 +993,45 @@ int yk_get_state(yk_ctx* c, double* x, double* v, double* vold, double* a)
     if (vold) CK(c, cudaMemcpyAsync(vold, c->vold, b, cudaMemcpyDeviceToHost, c->stream));
     if (a) CK(c, cudaMemcpyAsync(a, c->a, b, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
+    return YK_OK;
+}
+
+int yk_snapshot_wait(yk_ctx* c)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    if (!c->snap_pending) return YK_OK;
+    CK(c, cudaSetDevice(c->dev));
+    c->snap_pending = false;
+    CK(c, cudaEventSynchronize(c->snap_done));
+    return YK_OK;
+}
+
+int yk_snapshot_begin(yk_ctx* c, double* x, double* v, double* a)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    CK(c, cudaSetDevice(c->dev));
+    int rc = yk_snapshot_wait(c);           // one snapshot in flight at a time
+    if (rc) return rc;
+    if (!c->snap) {
+        CK(c, cudaMalloc(&c->snap, sizeof(double) * 9 * (size_t)c->n));
+        CK(c, cudaStreamCreateWithFlags(&c->snap_stream, cudaStreamNonBlocking));
+        CK(c, cudaEventCreateWithFlags(&c->snap_taken, cudaEventDisableTiming));
+        CK(c, cudaEventCreateWithFlags(&c->snap_done, cudaEventDisableTiming));
+    }
+    const size_t cnt = 3 * (size_t)c->n, b = sizeof(double) * cnt;
+    double* host[3] = {x, v, a};
+    const double* src[3] = {c->x, c->v, c->a};
+    // device-to-device on the engine's stream: ordered after every step already
+    // enqueued, and the next step may overwrite x, v, a as soon as it is done
+    for (int k = 0; k < 3; ++k)
+        if (host[k]) CK(c, cudaMemcpyAsync(c->snap + k * cnt, src[k], b, cudaMemcpyDeviceToDevice, c->stream));
+    CK(c, cudaEventRecord(c->snap_taken, c->stream));
+    // device-to-host on the side stream, overlapping the following steps
+    CK(c, cudaStreamWaitEvent(c->snap_stream, c->snap_taken, 0));
+    for (int k = 0; k < 3; ++k)
+        if (host[k]) CK(c, cudaMemcpyAsync(host[k], c->snap + k * cnt, b, cudaMemcpyDeviceToHost, c->snap_stream));
+    CK(c, cudaEventRecord(c->snap_done, c->snap_stream));
+    c->snap_pending = true;
     return YK_OK;
 }
 

@@ -114,6 +114,21 @@ class Engine:
         for k in range(3):
             self.params.xl[k] = float(xl[k])
 
+    # -- asynchronous snapshots (checkpoint / save_config) ------------------
+    def snapshot_begin(self, x=None, v=None, a=None):
+        """Start copying x, v, a (host float64 arrays of 3n, written in place)
+        from the device; returns at once.  The arrays hold the snapshot after
+        snapshot_wait()."""
+        for t in (x, v, a):
+            if t is not None and t.size != 3 * self.n:
+                raise ValueError("snapshot arrays hold 3*n doubles")
+        check(self._lib.yk_snapshot_begin(self._ctx, _ptr(x), _ptr(v), _ptr(a)), self._ctx)
+        self._snap_refs = (x, v, a)        # keep the targets alive while the copy runs
+
+    def snapshot_wait(self):
+        check(self._lib.yk_snapshot_wait(self._ctx), self._ctx)
+        self._snap_refs = None
+
     # -- gen_utils.f / strain.f on the device ------------------------------
     def ttot(self):
         out = C.c_double()
