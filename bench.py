@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--drift", type=int, default=0,
                     help="instead of the benchmark: run this many steps in FP64 and in mixed "
                          "precision and report the total-energy drift")
+    ap.add_argument("--kernel", choices=["auto", "rows", "pairs", "near"], default="auto",
+                    help="force kernel (default: the engine's automatic choice)")
     ap.add_argument("--drift-warmup", type=int, default=20,
                     help="warm-up groups of 100 steps (cancel_vcom + tnorm after each) before --drift")
     ap.add_argument("--ensemble-steps", type=int, default=100)
@@ -218,13 +220,18 @@ def device_uuid(dev):
 # ---------------------------------------------------------------------------
 # our arm
 
+KERNEL_CHOICE = [0]       # --kernel: 0 auto, 1 rows, 2 pairs, 3 near lists
+
+
 def time_engine(w, precision, steps, warmup, meas_every, dist, flush=True):
     """W untimed steps, then K timed steps; returns (ms_total, perf, launches)."""
     from yukawamd_b200 import abi
     from yukawamd_b200.engine import Engine, kernel_launch_count
     prec = abi.YK_PREC_MIXED if precision == "mixed" else abi.YK_PREC_FP64
     e = Engine(w, precision=prec, device=dist.local)
-    e.kernel_name = {1: "k_force_rows", 2: "k_force_pairs"}.get(e.tuning().force_kernel, "?")
+    if KERNEL_CHOICE[0]:
+        e.set_tuning(force_kernel=KERNEL_CHOICE[0])
+    e.kernel_name = {1: "k_force_rows", 2: "k_force_pairs", 3: "k_force_near"}.get(e.tuning().force_kernel, "?")
     e.accel(True)                                  # md.F:69, initial forces
     if warmup:
         e.run(warmup, meas_every, series=False)
@@ -564,6 +571,7 @@ def main():
             return 0
         print(json.dumps(run_reference(args)), flush=True)
         return 0
+    KERNEL_CHOICE[0] = {"auto": 0, "rows": 1, "pairs": 2, "near": 3}[args.kernel]
     dist = Dist()
     dist.init()
     try:

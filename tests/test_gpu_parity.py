@@ -66,7 +66,9 @@ def check_accel(orc, w, prec, meas, mix_mode=abi.YK_MIX_COMPAT, tuning=None):
 
 KERNELS = {"rows": dict(force_kernel=abi.KERNEL_ROWS),
            "pairs": dict(force_kernel=abi.KERNEL_PAIRS),
-           "pairs-unsorted-seg3": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, pair_seg=3)}
+           "pairs-unsorted-seg3": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, pair_seg=3),
+           "near": dict(force_kernel=abi.KERNEL_NEAR),
+           "near-unsorted-seg3": dict(force_kernel=abi.KERNEL_NEAR, sort_every=-1, pair_seg=3)}
 
 
 @pytest.mark.parametrize("kern", list(KERNELS))
@@ -77,7 +79,7 @@ def test_accel_matches_oracle(gpu, orc, kind, n, meas, prec, kern):
     check_accel(orc, workload(kind, n, 100 + n), prec, meas, tuning=KERNELS[kern])
 
 
-@pytest.mark.parametrize("kern", ["rows", "pairs"])
+@pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
 @pytest.mark.parametrize("n", [1, 2, 3, 17, 127, 128, 129, 255, 257])
 @pytest.mark.parametrize("kind", ["pure", "mix", "nn"])
 def test_ragged_sizes(gpu, orc, kind, n, kern):
@@ -86,7 +88,7 @@ def test_ragged_sizes(gpu, orc, kind, n, kern):
     check_accel(orc, w, abi.YK_PREC_FP64, False, tuning=KERNELS[kern])
 
 
-@pytest.mark.parametrize("kern", ["rows", "pairs"])
+@pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
 @pytest.mark.parametrize("mode", [abi.YK_MIX_COMPAT, abi.YK_MIX_FIXED], ids=["compat", "fixed"])
 def test_mix_last_particle_mode(gpu, orc, mode, kern):
     check_accel(orc, workload("mix", 513, 5), abi.YK_PREC_FP64, False, mix_mode=mode,
@@ -167,7 +169,7 @@ def test_newton_steps_match_oracle(gpu, orc, kind):
     assert rel(s.px, s_ref.px) <= 1e-11
 
 
-@pytest.mark.parametrize("kern", ["rows", "pairs"])
+@pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
 def test_run_graph_equals_newton_loop(gpu, prec, kern):
     """yk_run (CUDA graphs, Morton re-sorts inside) is bit-identical to the

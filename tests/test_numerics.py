@@ -1,0 +1,100 @@
+"""The mixed form's FP32 exp(-t) (exp_neg_f32 in yukawamd_b200/csrc/yk_common.cuh).
+
+1. The degree-6 polynomial for 2^f on [-1/2, 1/2] with the source's float32
+   constants is within 2e-8 (0.3 ulp) relative of 2^f; a fresh fit of the
+   same form (relative-error least squares with Lawson reweighting on 4001
+   Chebyshev nodes) reaches 2.5e-9 in exact arithmetic, so the degree leaves
+   the error to the float32 rounding.  (High-order coefficients of such fits
+   are ill-conditioned, so they are not compared one by one.)
+2. A float32 restatement of the device function (magic-number rounding, the
+   Cody-Waite split of t*log2(e), Horner with fused multiply-adds, exponent
+   scaling through the bits) stays within 2 ulp of exp(-t) for t in [0, 80],
+   which covers every argument of the pair terms (mu r <= mu r_c, and
+   r^2 / (2 Lambda) <= rncut^2 / (2 Lambda) = 53 for the default HPP cutoff).
+"""
+import re
+import os
+
+import numpy as np
+
+SRC = os.path.join(os.path.dirname(__file__), "..", "yukawamd_b200", "csrc", "yk_common.cuh")
+
+
+def source_coefficients():
+    text = open(SRC).read()
+    body = text[text.index("float exp_neg_f32"):]
+    body = body[:body.index("}")]
+    first = float(re.search(r"float p = ([0-9.eE+-]+)f;", body).group(1))
+    rest = [float(c) for c in re.findall(r"p = fmaf\(p, f, ([0-9.eE+-]+)f\);", body)]
+    return [first] + rest          # highest degree first
+
+
+def lawson_fit(deg=6, nodes=4001, iters=60):
+    k = np.arange(nodes)
+    x = 0.5 * np.cos(np.pi * (k + 0.5) / nodes)
+    y = np.exp2(x)
+    V = np.vander(x, deg + 1)                  # highest degree first
+    w = np.ones(nodes)
+    for _ in range(iters):
+        A = V * (w / y)[:, None]
+        c, *_ = np.linalg.lstsq(A, w, rcond=None)
+        e = np.abs(V @ c / y - 1.0)
+        w = w * e
+        w = w / w.sum() * nodes
+    return c, np.max(np.abs(V @ c / y - 1.0))
+
+
+def test_coefficients_are_the_fit():
+    c_src = np.array(source_coefficients())
+    assert len(c_src) == 7
+    _c_fit, err = lawson_fit()
+    assert err < 2.5e-9
+    x = np.linspace(-0.5, 0.5, 20001)
+    p_src = np.polyval(c_src, x)
+    assert np.max(np.abs(p_src / np.exp2(x) - 1.0)) < 2e-8
+
+
+def _fma32(a, b, c):
+    # the exact product of two floats fits a double; one rounding to float32
+    return np.float32(np.float64(a) * np.float64(b) + np.float64(c))
+
+
+def exp_neg_f32(t):
+    f32 = np.float32
+    L2E_HI = f32(1.44269502162933349609375)
+    L2E_LO = f32(1.925963033500011079e-8)
+    MAGIC = f32(12582912.0)
+    t = f32(t)
+    yh = f32(-t * L2E_HI)
+    yl = _fma32(-t, L2E_HI, -yh)
+    yl = _fma32(-t, L2E_LO, yl)
+    kb = f32(yh + MAGIC)
+    k = f32(kb - MAGIC)
+    f = f32(f32(yh - k) + yl)
+    c = source_coefficients()
+    p = f32(c[0])
+    for cm in c[1:]:
+        p = _fma32(p, f, f32(cm))
+    ki = int(np.array(kb, dtype=np.float32).view(np.int32)) - 0x4B400000
+    if k < -125.0:
+        return f32(0.0)
+    bits = int(np.array(p, dtype=np.float32).view(np.int32)) + (ki << 23)
+    return np.array(bits, dtype=np.int32).view(np.float32).item()
+
+
+def test_restated_exp_within_two_ulp():
+    rng = np.random.default_rng(3)
+    ts = np.concatenate([np.linspace(0.0, 80.0, 801), rng.uniform(0.0, 20.0, 600),
+                         [0.0, 1e-8, 0.5, 0.6931472, 1.0, 10.0, 53.0, 80.0]])
+    worst = 0.0
+    for t in ts:
+        got = exp_neg_f32(t)
+        ref = np.exp(-np.float64(np.float32(t)))
+        ulp = np.spacing(np.float32(ref))
+        worst = max(worst, abs(got - ref) / ulp)
+    assert worst <= 2.0, worst
+
+
+def test_underflow_flushes_to_zero():
+    assert exp_neg_f32(100.0) == 0.0
+    assert exp_neg_f32(1e5) == 0.0

@@ -118,6 +118,7 @@ class YkTuning(C.Structure):
 KERNEL_AUTO = 0
 KERNEL_ROWS = 1
 KERNEL_PAIRS = 2
+KERNEL_NEAR = 3
 
 
 class YkPerf(C.Structure):

@@ -8,8 +8,8 @@
 //  * compensated FP32 accumulation (Knuth two-sum) for the mixed form.
 //  * an FP32 exp(-t) built from Cody-Waite reduction and a polynomial for
 //    2^f on [-1/2, 1/2] (relative-error least-squares fit with Lawson
-//    reweighting on 4001 Chebyshev nodes; tests/test_numerics.py re-runs the
-//    fit and checks the error bound).
+//    reweighting on Chebyshev nodes; tests/test_numerics.py checks the
+//    polynomial's error bound and a float32 restatement of the function).
 #pragma once
 
 #include <cstdint>
@@ -83,6 +83,21 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
     return false;
 }
 
+// As mbar_wait_bounded, for the warps of a CTA that do not meet at a block
+// barrier between waits: a waiter also gives up as soon as another thread has
+// raised *abort, and one that times out raises it.
+__device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, unsigned parity, unsigned* err,
+                                                    volatile int* abort)
+{
+    for (long long it = 0; it < SPIN_LIMIT; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63) == 63 && *abort) return false;
+    }
+    atomicOr(err, ERR_TIMEOUT);
+    *abort = 1;
+    return false;
+}
+
 // ---- reductions ----------------------------------------------------------
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -152,16 +167,21 @@ struct kf32 {
 // product's rounding error recovered by an FMA (Cody-Waite style), so f is
 // accurate to ~1e-9 absolute; 2^f comes from a degree-6 polynomial fitted
 // on [-1/2, 1/2] (2e-9 relative in exact arithmetic, 1e-7 = 1.7 ulp with
-// FP32 Horner rounding); 2^k is applied through
-// the exponent bits.  Results below 2^-126 flush to zero.
+// FP32 Horner rounding); 2^k is applied through the exponent bits.  k is
+// rounded with the 1.5*2^23 add (round to nearest even, as rintf) and read
+// back as an integer from the sum's low mantissa bits, so the function uses
+// only FMA-pipe and integer instructions (no conversion or rounding unit).
+// Valid for t < 2.9e6; results below 2^-126 flush to zero.
 __device__ __forceinline__ float exp_neg_f32(float t)
 {
     const float L2E_HI = 1.44269502162933349609375f;      // float(log2 e)
     const float L2E_LO = 1.925963033500011079e-8f;       // log2 e - L2E_HI
+    const float MAGIC = 12582912.0f;                      // 1.5 * 2^23
     float yh = -t * L2E_HI;
     float yl = fmaf(-t, L2E_HI, -yh);                    // exact error of -t*L2E_HI
     yl = fmaf(-t, L2E_LO, yl);
-    float k = rintf(yh);
+    const float kb = __fadd_rn(yh, MAGIC);               // k in the low mantissa bits
+    const float k = __fsub_rn(kb, MAGIC);
     float f = (yh - k) + yl;                             // yh - k is exact
     // 2^f = sum c_m f^m, c_m fitted to 2^f on [-0.5, 0.5]
     float p = 1.5353360504377633e-4f;
@@ -171,7 +191,7 @@ __device__ __forceinline__ float exp_neg_f32(float t)
     p = fmaf(p, f, 2.4022647738456726e-1f);
     p = fmaf(p, f, 6.9314718246459961e-1f);
     p = fmaf(p, f, 1.0f);
-    int ki = (int)k;
+    const int ki = __float_as_int(kb) - 0x4B400000;
     float r = __int_as_float(__float_as_int(p) + (ki << 23));
     return (k < -125.f) ? 0.f : r;
 }

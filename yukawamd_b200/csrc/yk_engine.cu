@@ -24,6 +24,7 @@
 #include "yk_force.cuh"
 #include "yk_internal.h"
 #include "yk_pairs.cuh"
+#include "yk_near.cuh"
 #include "yk_sort.cuh"
 #include "yk_thermo.cuh"
 #include "yk_verlet.cuh"
@@ -103,7 +104,7 @@ struct yk_ctx {
     StepArgs sa{};
     FinishArgs fz_base{};
     int nfb = 0, nvb = 0;
-    int kernel = 2;                 // 1 rows, 2 pairs (resolved, never 0)
+    int kernel = 2;                 // 1 rows, 2 pairs, 3 near lists (resolved, never 0)
     int kernel_req = 0;             // as requested (0 = auto)
     int seg = DEFAULT_SEG;
     int sort_every = DEFAULT_SORT_EVERY;
@@ -338,7 +339,7 @@ static int resolve_kernel(yk_ctx* c)
 {
     int k = c->kernel_req;
     if (k == 0) k = (pair_scratch_bytes(c->n, c->seg) <= PAIR_SCRATCH_BUDGET) ? 2 : 1;
-    if (k == 2) {
+    if (k == 2 || k == 3) {
         int rc = setup_pairs(c);
         if (rc) return rc;
     } else {
@@ -395,17 +396,23 @@ static int launch_force_t(yk_ctx* c)
             c->pos, c->posf, c->perm, c->aii, c->fa, c->a, c->fpart, c->err);
         return 1;
     }
-    static int grid = 0;
+    static int grid = 0, grid_near = 0;
     if (grid == 0) {
-        int per_sm = 0, sms = 0;
+        int per_sm = 0, per_sm_near = 0, sms = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs<SIM, PREC, MEAS>, PB, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_near, k_force_near<SIM, PREC, MEAS>, PB, 0);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
         grid = std::max(1, per_sm) * std::max(1, sms);
+        grid_near = std::max(1, per_sm_near) * std::max(1, sms);
     }
     cudaMemsetAsync(c->job_counter, 0, sizeof(int), c->stream);
-    const int g = std::min(grid, c->pj.njobs);
-    k_force_pairs<SIM, PREC, MEAS><<<g, PB, 0, c->stream>>>(c->pos, c->posf, c->pj, c->job_counter,
-                                                            c->fa, c->Si, c->Sj, c->Sm, c->err);
+    if (c->kernel == 3) {
+        k_force_near<SIM, PREC, MEAS><<<std::min(grid_near, c->pj.njobs), PB, 0, c->stream>>>(
+            c->pos, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+    } else {
+        k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
+            c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+    }
     k_combine<SIM><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->Si, c->Sj, c->pj, c->perm, c->zii,
                                                               c->aii, c->fa, c->a);
     return 2;
@@ -448,7 +455,7 @@ static int enqueue_finish(yk_ctx* c, bool meas, int kin_mode, bool series)
     const bool has_force = c->p.sim_type != YK_SIM_BFIELD;
     z.force_mode = has_force ? 1 : 0;
     z.do_meas = meas ? 1 : 0;
-    if (c->kernel == 2) {
+    if (c->kernel >= 2) {
         z.nfp = (has_force && meas) ? c->pj.njobs : 0;
         z.half = 1.0;                   // each unique pair counted once
     } else {
@@ -457,7 +464,7 @@ static int enqueue_finish(yk_ctx* c, bool meas, int kin_mode, bool series)
     }
     z.kin_mode = kin_mode;
     z.nkp = (kin_mode == 2) ? c->nvb : 0;
-    k_finish<<<1, 256, 0, c->stream>>>(c->kernel == 2 ? c->Sm : c->fpart, c->kpart, z, c->a, c->ds,
+    k_finish<<<1, 256, 0, c->stream>>>(c->kernel >= 2 ? c->Sm : c->fpart, c->kpart, z, c->a, c->ds,
                                        series ? c->series : nullptr, c->series_idx);
     return 1;
 }
@@ -847,7 +854,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
 int yk_get_tuning(yk_ctx* c, yk_tuning* out)
 {
     if (!c || !out) return fail(c, YK_ERR_ARG, "ctx and out are required");
-    out->force_kernel = c->kernel;          // the resolved kernel (1 rows, 2 pairs)
+    out->force_kernel = c->kernel;          // the resolved kernel (1 rows, 2 pairs, 3 near lists)
     out->pair_seg = c->seg;
     out->sort_every = c->sort_every;
     out->graph_steps = c->graph_steps;
@@ -857,7 +864,7 @@ int yk_get_tuning(yk_ctx* c, yk_tuning* out)
 int yk_set_tuning(yk_ctx* c, const yk_tuning* t)
 {
     if (!c || !t) return fail(c, YK_ERR_ARG, "ctx and tuning are required");
-    if (t->force_kernel < 0 || t->force_kernel > 2) return fail(c, YK_ERR_ARG, "force_kernel must be 0..2");
+    if (t->force_kernel < 0 || t->force_kernel > 3) return fail(c, YK_ERR_ARG, "force_kernel must be 0..3");
     if (t->pair_seg < 0 || t->graph_steps < 0 || t->sort_every < -1)
         return fail(c, YK_ERR_ARG, "bad tuning values");
     CK(c, cudaSetDevice(c->dev));

@@ -141,13 +141,11 @@ struct PairOut {
 };
 
 // ---- one pair, FP64 -------------------------------------------------------
+// phys64: the pair terms from a minimum-image displacement already in o.dx,
+// o.dy, o.dz; wi, wj are the species / charge words of the two particles.
 template <int SIM, bool MEAS>
-__device__ __forceinline__ void pair64(const ForceArgs& fa, const double4& pi, const double4& pj,
-                                       bool valid, PairOut<double>& o)
+__device__ __forceinline__ void phys64(const ForceArgs& fa, double wi, double wj, bool valid, PairOut<double>& o)
 {
-    o.dx = min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]);
-    o.dy = min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]);
-    o.dz = min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]);
     const double r2 = o.dx * o.dx + o.dy * o.dy + o.dz * o.dz;
     o.fs = 0.0;
     o.u = 0.0;
@@ -170,7 +168,7 @@ __device__ __forceinline__ void pair64(const ForceArgs& fa, const double4& pi, c
         if (!valid) return;
         if (fa.nuclear_on && r2 <= fa.rn2) {
             const double e = exp(-(r2 * fa.xp2i));
-            const double B = (pi.w == pj.w) ? fa.bpc : fa.bmc;
+            const double B = (wi == wj) ? fa.bpc : fa.bmc;
             const double fn = fa.xpi * (fa.aa2 * e + B) * e;
             o.fs = fn;
             if constexpr (MEAS) {
@@ -179,7 +177,7 @@ __device__ __forceinline__ void pair64(const ForceArgs& fa, const double4& pi, c
             }
             o.hit = true;
         }
-        if (fa.coulomb_on && pi.w == 1.0 && pj.w == 1.0 && r2 <= fa.rc2) {
+        if (fa.coulomb_on && wi == 1.0 && wj == 1.0 && r2 <= fa.rc2) {
             const double rinv = rsqrt(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;
@@ -195,14 +193,21 @@ __device__ __forceinline__ void pair64(const ForceArgs& fa, const double4& pi, c
     }
 }
 
-// ---- one pair, mixed ---------------------------------------------------------
 template <int SIM, bool MEAS>
-__device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, const double4& pj,
-                                       bool valid, PairOut<float>& o)
+__device__ __forceinline__ void pair64(const ForceArgs& fa, const double4& pi, const double4& pj,
+                                       bool valid, PairOut<double>& o)
 {
-    o.dx = __double2float_rn(min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]));
-    o.dy = __double2float_rn(min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]));
-    o.dz = __double2float_rn(min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]));
+    o.dx = min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]);
+    o.dy = min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]);
+    o.dz = min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]);
+    phys64<SIM, MEAS>(fa, pi.w, pj.w, valid, o);
+}
+
+// ---- one pair, mixed ---------------------------------------------------------
+// phys32: the FP32 pair terms from the cast displacement in o.dx, o.dy, o.dz.
+template <int SIM, bool MEAS>
+__device__ __forceinline__ void phys32(const ForceArgs& fa, double wi, double wj, bool valid, PairOut<float>& o)
+{
     const float r2 = fmaf(o.dx, o.dx, fmaf(o.dy, o.dy, o.dz * o.dz));
     o.fs = 0.f;
     o.u = 0.f;
@@ -225,7 +230,7 @@ __device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, c
         if (!valid) return;
         if (fa.nuclear_on && r2 <= fa.rn2f) {
             const float e = exp_neg_f32(r2 * fa.xp2if);
-            const float B = (pi.w == pj.w) ? fa.bpcf : fa.bmcf;
+            const float B = (wi == wj) ? fa.bpcf : fa.bmcf;
             const float fn = fa.xpif * fmaf(fa.aa2f, e, B) * e;
             o.fs = fn;
             if constexpr (MEAS) {
@@ -234,7 +239,7 @@ __device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, c
             }
             o.hit = true;
         }
-        if (fa.coulomb_on && pi.w == 1.0 && pj.w == 1.0 && r2 <= fa.rc2f) {
+        if (fa.coulomb_on && wi == 1.0 && wj == 1.0 && r2 <= fa.rc2f) {
             const float rinv = rsqrt_f32(r2);
             const float r = r2 * rinv;
             const float mr = fa.xmucf * r;
@@ -247,6 +252,71 @@ __device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, c
             }
             o.hit = true;
         }
+    }
+}
+
+template <int SIM, bool MEAS>
+__device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, const double4& pj,
+                                       bool valid, PairOut<float>& o)
+{
+    o.dx = __double2float_rn(min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]));
+    o.dy = __double2float_rn(min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]));
+    o.dz = __double2float_rn(min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]));
+    phys32<SIM, MEAS>(fa, pi.w, pj.w, valid, o);
+}
+
+// ---- one ion pair without branches ------------------------------------------
+// The screened-Coulomb terms of phys64 / phys32 for a pair that sel says the
+// screen selected; computed unconditionally (a placeholder r^2 = 1 for pairs
+// that do not interact) and masked, so that several pairs' chains can be
+// interleaved by the compiler.  The FP64 form takes the reference's minimum
+// image on integer compares; the mixed form takes it on FP64 compares, which
+// keep it off the integer pipe that the mixed path already loads.
+__device__ __forceinline__ double min_image_cmp(double d, double L, double hL)
+{
+    double s = 0.0;
+    if (d > hL) s = -L;
+    else if (d < -hL) s = L;
+    return __dadd_rn(d, s);
+}
+
+template <int PREC, bool MEAS>
+__device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& pi, const double4& pj, bool sel,
+                                            PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o)
+{
+    if constexpr (PREC == PREC_FP64) {
+        o.dx = min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]);
+        o.dy = min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]);
+        o.dz = min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]);
+        const double r2 = o.dx * o.dx + o.dy * o.dy + o.dz * o.dz;
+        const bool hit = sel && r2 <= fa.rc2;
+        const double r2s = hit ? r2 : 1.0;
+        const double rinv = rsqrt(r2s);
+        const double r = r2s * rinv;
+        const double mr = fa.xmuc * r;
+        const double er = exp(-mr) * rinv;
+        const double fs = (1.0 + mr) * er * (rinv * rinv);
+        o.fs = hit ? fs : 0.0;
+        o.u = (MEAS && hit) ? er - fa.evcut : 0.0;
+        o.w = (MEAS && hit) ? fs * r2 : 0.0;
+        o.hit = hit;
+    } else {
+        const double hx = 0.5 * fa.xl[0], hy = 0.5 * fa.xl[1], hz = 0.5 * fa.xl[2];
+        o.dx = __double2float_rn(min_image_cmp(__dsub_rn(pi.x, pj.x), fa.xl[0], hx));
+        o.dy = __double2float_rn(min_image_cmp(__dsub_rn(pi.y, pj.y), fa.xl[1], hy));
+        o.dz = __double2float_rn(min_image_cmp(__dsub_rn(pi.z, pj.z), fa.xl[2], hz));
+        const float r2 = fmaf(o.dx, o.dx, fmaf(o.dy, o.dy, o.dz * o.dz));
+        const bool hit = sel && r2 <= fa.rc2f;
+        const float r2s = hit ? r2 : 1.0f;
+        const float rinv = rsqrt_f32(r2s);
+        const float r = r2s * rinv;
+        const float mr = fa.xmucf * r;
+        const float er = exp_neg_f32(mr) * rinv;
+        const float fs = (1.0f + mr) * er * (rinv * rinv);
+        o.fs = hit ? fs : 0.f;
+        o.u = (MEAS && hit) ? er - fa.evcutf : 0.f;
+        o.w = (MEAS && hit) ? fs * r2 : 0.f;
+        o.hit = hit;
     }
 }
 
@@ -292,6 +362,39 @@ struct TargetAcc<PREC_FP64, MEAS> {
     }
 };
 
+// Plain sum of a few pair terms (one group of sources) before they enter the
+// compensated per-target sum of the mixed form.
+template <int PREC, bool MEAS>
+struct GroupSum {
+    using R = std::conditional_t<PREC == PREC_FP64, double, float>;
+    R f[3];
+    R s[MEAS ? NSCAL : 1];
+    __device__ __forceinline__ void zero()
+    {
+        f[0] = f[1] = f[2] = (R)0;
+#pragma unroll
+        for (int k = 0; k < (MEAS ? NSCAL : 1); ++k) s[k] = (R)0;
+    }
+    __device__ __forceinline__ void add(const PairOut<R>& o, R weight)
+    {
+        const R fs = o.fs * weight;
+        const R fx = fs * o.dx, fy = fs * o.dy, fz = fs * o.dz;
+        f[0] += fx;
+        f[1] += fy;
+        f[2] += fz;
+        if constexpr (MEAS) {
+            s[0] += o.u * weight;
+            s[1] += o.w * weight;
+            s[2] += o.dx * fx;
+            s[3] += o.dx * fy;
+            s[4] += o.dx * fz;
+            s[5] += o.dy * fy;
+            s[6] += o.dy * fz;
+            s[7] += o.dz * fz;
+        }
+    }
+};
+
 template <bool MEAS>
 struct TargetAcc<PREC_MIXED, MEAS> {
     cf32 f[3];
@@ -318,6 +421,17 @@ struct TargetAcc<PREC_MIXED, MEAS> {
             s[5].add(o.dy * fy);
             s[6].add(o.dy * fz);
             s[7].add(o.dz * fz);
+        }
+    }
+    // a group's plain FP32 sum enters the compensated sums as one term
+    __device__ __forceinline__ void add_group(const GroupSum<PREC_MIXED, MEAS>& g)
+    {
+        f[0].add(g.f[0]);
+        f[1].add(g.f[1]);
+        f[2].add(g.f[2]);
+        if constexpr (MEAS) {
+#pragma unroll
+            for (int k = 0; k < NSCAL; ++k) s[k].add(g.s[k]);
         }
     }
     __device__ __forceinline__ double force(int k) const { return f[k].value(); }

@@ -64,13 +64,15 @@ __device__ __forceinline__ double to_f64(real_t<PREC> v)
 
 // Reduce-scatter of four 3-vectors held in lane-swizzled slots (slot q of
 // lane L belongs to source q ^ sw(L)).  On return t[] holds the warp-wide sum
-// for source sw(L).
-__device__ __forceinline__ void reduce_scatter4(double (&r)[4][3], double (&t)[3])
+// for source sw(L).  T is double for the FP64 form and float for the mixed
+// form (whose reaction terms are FP32 products).
+template <typename T>
+__device__ __forceinline__ void reduce_scatter4(T (&r)[4][3], T (&t)[3])
 {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const double a0 = r[0][c] + __shfl_xor_sync(0xffffffffu, r[2][c], 16);
-        const double a1 = r[1][c] + __shfl_xor_sync(0xffffffffu, r[3][c], 16);
+        const T a0 = r[0][c] + __shfl_xor_sync(0xffffffffu, r[2][c], 16);
+        const T a1 = r[1][c] + __shfl_xor_sync(0xffffffffu, r[3][c], 16);
         t[c] = a0 + __shfl_xor_sync(0xffffffffu, a1, 8);
     }
 #pragma unroll
@@ -107,36 +109,60 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
         m &= ok;
     }
     if (!__any_sync(0xffffffffu, m != 0)) return;
-    double r[4][3];
+    R_t r[4][3];
+    GroupSum<PREC, MEAS> gs;             // the mixed form adds the group, then compensates
+    gs.zero();
     bool any = false;
+    if constexpr (SIM == SIM_PURE || SIM == SIM_MIX) {
+        // Ions: the 4 pairs are evaluated without branches, so that their
+        // independent instruction chains interleave; a pair the screen did
+        // not select, or outside r_c, gets zero terms.
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const int src = jj ^ sw;
+            const double4 pjv = tl[j0 + src];
+            PairOut<R_t> o;
+            ion_pair_nb<PREC, MEAS>(fa, pi, pjv, ((m >> src) & 1u) != 0, o);
+            if constexpr (PREC == PREC_FP64) acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
+            else gs.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
+            const R_t fsj = o.fs * wi;               // 0 unless the pair interacts
+            r[jj][0] = fsj * o.dx;
+            r[jj][1] = fsj * o.dy;
+            r[jj][2] = fsj * o.dz;
+            any |= o.hit;
+        }
+    } else {
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) {
         const int src = jj ^ sw;
-        r[jj][0] = r[jj][1] = r[jj][2] = 0.0;
+        r[jj][0] = r[jj][1] = r[jj][2] = (R_t)0;
         if ((m >> src) & 1u) {
             const double4 pjv = tl[j0 + src];
             PairOut<R_t> o;
             pair_eval<SIM, PREC, MEAS>(fa, pi, pjv, true, o);
             if (o.hit) {
-                acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
+                if constexpr (PREC == PREC_FP64) acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
+                else gs.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
                 // reaction on j: Z_i fs d (int_ion_mix.f:180)
                 const R_t fsj = o.fs * wi;
-                r[jj][0] = to_f64<PREC>(fsj * o.dx);
-                r[jj][1] = to_f64<PREC>(fsj * o.dy);
-                r[jj][2] = to_f64<PREC>(fsj * o.dz);
+                r[jj][0] = fsj * o.dx;
+                r[jj][1] = fsj * o.dy;
+                r[jj][2] = fsj * o.dz;
                 any = true;
             }
         }
     }
+    }
+    if constexpr (PREC == PREC_MIXED) acc.add_group(gs);
     if (__any_sync(0xffffffffu, any)) {
-        double t[3];
+        R_t t[3];
         reduce_scatter4(r, t);
         const int lane = threadIdx.x & 31;
         const int jl = j0 + sw;
         if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
-            my_acc[3 * jl] -= t[0];
-            my_acc[3 * jl + 1] -= t[1];
-            my_acc[3 * jl + 2] -= t[2];
+            my_acc[3 * jl] -= (double)t[0];
+            my_acc[3 * jl + 1] -= (double)t[1];
+            my_acc[3 * jl + 2] -= (double)t[2];
         }
     }
 }
@@ -145,9 +171,11 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
 struct PairSmem {
     double4 tile[2][PB];                  // FP64 source tiles (TMA)
     float tilef[2][4 * SHADOW_TILE];      // FP32 shadow source tiles (TMA)
-    double acc_j[2][PWARPS][PB * 3];      // per-warp reaction rows, double-buffered by tile
+    double acc_j[2][PWARPS][PB * 3];      // per-warp reaction rows, one set per tile stage
     double red[32 * NSCAL];               // block reduction scratch
     uint64_t bar[2];                      // one mbarrier per tile stage
+    int done[2];                          // warps finished with the stage's tile
+    int abort;                            // a tile copy timed out: every warp leaves
     int s_job;
 };
 
@@ -163,15 +191,23 @@ struct BoxView {
 
 __device__ __forceinline__ void pairs_smem_init(PairSmem& sm)
 {
+    // The ion path evaluates all 4 pairs of a group and masks the terms
+    // (ion_pair_nb), so it also reads the slots of a partial tile that no copy
+    // filled.  Zero them once: from then on every slot holds a finite position
+    // (zero, or one left by an earlier tile) and a masked pair yields 0, not NaN.
+    for (int k = threadIdx.x; k < 2 * PB; k += blockDim.x) (&sm.tile[0][0])[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int k = threadIdx.x; k < 2 * 4 * SHADOW_TILE; k += blockDim.x) (&sm.tilef[0][0])[k] = 0.f;
     if (threadIdx.x == 0) {
         mbar_init(&sm.bar[0], 1);
         mbar_init(&sm.bar[1], 1);
         fence_mbar_init();
+        sm.done[0] = sm.done[1] = 0;
+        sm.abort = 0;
     }
     __syncthreads();
 }
 
-// Load source tile C of box bx into stage qq & 1 (thread 0 only).
+// Load source tile C of box bx into stage qq & 1 (one thread).
 __device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int C, unsigned qq)
 {
     const int j0 = C * PB;
@@ -189,6 +225,15 @@ __device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int
 // consumed (stage and mbarrier parity).  Writes Si / Sj rows of the box and,
 // when measuring, the job's 8 sums to sm_row.  Returns false if a tile copy
 // timed out (the CTA must then leave).
+//
+// The warps do not meet at a block barrier between tiles.  A warp that has
+// finished tile C counts itself in done[stage]; the last of the four sums the
+// four warps' reaction rows of the tile into the unit's Sj row (in warp
+// order, so the result does not depend on which warp came last) and then
+// issues the copy of tile C+2 into the freed stage.  A warp starts tile C+2
+// only after that copy has landed, so it never overwrites rows that are
+// still being summed.  Warps may thus run up to one tile apart, which absorbs
+// the uneven work of the four target groups.
 template <int SIM, int PREC, bool MEAS>
 __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, const BoxView& bx, int R, int sg,
                                           double* __restrict__ sm_row, unsigned* __restrict__ err,
@@ -206,34 +251,28 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
     const ScreenI si = load_screen_i(bx.posf, active ? i : 0);
     const R_t wi = (SIM == SIM_MIX) ? (R_t)pi.w : (R_t)1;   // Z_i of the reaction
     const bool all_active = (R + 1) * PB <= n;
+    const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
     TargetAcc<PREC, MEAS> acc;
     acc.zero();
 
+    // both stages are free: every warp has passed the block barrier that
+    // handed out this job
     if (tid == 0) {
         pairs_issue(sm, bx, C0, q);
         if (C0 + 1 < C1) pairs_issue(sm, bx, C0 + 1, q + 1);
     }
+    const unsigned q0 = q;
     for (int C = C0; C < C1; ++C, ++q) {
         const int st = q & 1;
-        // zero this tile's accumulator rows; the other buffer may still be
-        // read by threads finishing the previous tile's sum
-#pragma unroll
-        for (int w = 0; w < PWARPS; ++w) {
-            sm.acc_j[st][w][3 * tid] = 0.0;
-            sm.acc_j[st][w][3 * tid + 1] = 0.0;
-            sm.acc_j[st][w][3 * tid + 2] = 0.0;
-        }
-        const bool ok = mbar_wait_bounded(&sm.bar[st], (q >> 1) & 1u, err);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0 && C + 1 < C1) mbar_wait_bounded(&sm.bar[st ^ 1], ((q + 1) >> 1) & 1u, err);
-            return false;
-        }
+        if (!mbar_wait_abortable(&sm.bar[st], (q >> 1) & 1u, err, &sm.abort)) break;
         const int jlim = min(PB, n - C * PB);
         const bool diag = (C == R);
         const double4* tl = sm.tile[st];
         const float* tlf = sm.tilef[st];
         double* my_acc = sm.acc_j[st][warp];
-        const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
+#pragma unroll
+        for (int k = lane; k < PB * 3; k += 32) my_acc[k] = 0.0;
+        __syncwarp();
         if (!diag && jlim == PB && all_active) {
             for (int j0 = 0; j0 < PB; j0 += 4)
                 pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active, tid, sw,
@@ -243,18 +282,29 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
                 pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active, tid, sw,
                                                   acc, my_acc);
         }
-        __syncthreads();                  // tile done: stage st reusable, rows complete
-        if (tid == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2);
-        // source-side partial of unit (R, C): the warp rows in fixed order
-        double* dj = bx.Sj + ((size_t)tri_index(C, R) * PB + tid) * 3;
+        // this warp is done with the tile: the last warp reduces and refills
+        __threadfence_block();
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) last = atomicAdd(&sm.done[st], 1) == PWARPS - 1;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last) {
+            __threadfence_block();
+            if (lane == 0) sm.done[st] = 0;
+            double* dj = bx.Sj + (size_t)tri_index(C, R) * PB * 3;
+#pragma unroll 4
+            for (int k = lane; k < PB * 3; k += 32) {
+                double v = sm.acc_j[st][0][k];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            double v = sm.acc_j[st][0][3 * tid + c];
-#pragma unroll
-            for (int w = 1; w < PWARPS; ++w) v += sm.acc_j[st][w][3 * tid + c];
-            dj[c] = v;
+                for (int w = 1; w < PWARPS; ++w) v += sm.acc_j[st][w][k];
+                dj[k] = v;
+            }
+            __syncwarp();
+            if (lane == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2);
         }
     }
+    q = q0 + (unsigned)(C1 - C0);
+    if (__syncthreads_or(sm.abort)) return false;
     // target-side partial of job (R, s)
     double* di = bx.Si + (((size_t)R * bx.nseg_max + sg) * PB + tid) * 3;
     di[0] = acc.force(0);

@@ -21,6 +21,9 @@ import time
 from . import abi
 
 CANDIDATES = [
+    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=8, sort_every=50),
+    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=4, sort_every=50),
+    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=16, sort_every=50),
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=50),
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=4, sort_every=50),
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=16, sort_every=50),
