@@ -69,7 +69,7 @@ __global__ void k_b_morton(const double* __restrict__ x, const int* __restrict__
     const int cx = min(max((int)(x[3 * i] * (1024.0 / L[0])), 0), 1023);
     const int cy = min(max((int)(x[3 * i + 1] * (1024.0 / L[1])), 0), 1023);
     const int cz = min(max((int)(x[3 * i + 2] * (1024.0 / L[2])), 0), 1023);
-    const unsigned m = spread10(cx) | (spread10(cy) << 1) | (spread10(cz) << 2);
+    const unsigned m = hilbert10(cx, cy, cz);
     keys[i] = ((unsigned long long)r << 30) | m;
     idx[i] = i;
 }

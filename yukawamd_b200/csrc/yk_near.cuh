@@ -51,43 +51,6 @@ struct NearSmem {
     int s_job;
 };
 
-__device__ __forceinline__ float warp_minf(float v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-__device__ __forceinline__ float warp_maxf(float v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// Bounding box of a warp's active targets and the FP32 constants of the
-// classification.
-struct WarpBox {
-    float lo[3], hi[3];
-    bool any, has_p;                 // any active target; any proton target (nucleons)
-};
-
-__device__ __forceinline__ WarpBox warp_box(const double4& pi, bool active)
-{
-    WarpBox b;
-    const float inf = __int_as_float(0x7f800000);
-    const double c[3] = {pi.x, pi.y, pi.z};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float v = __double2float_rn(c[k]);
-        b.lo[k] = warp_minf(active ? v : inf);
-        b.hi[k] = warp_maxf(active ? v : -inf);
-    }
-    b.any = __any_sync(0xffffffffu, active);
-    b.has_p = __any_sync(0xffffffffu, active && pi.w == 1.0);
-    return b;
-}
-
 // Classify source pj against the warp box.  Returns true if some target of
 // the box may be within the screening radius; sets the per-axis image shift
 // (in units of L) and amb if any axis straddles +-L/2.

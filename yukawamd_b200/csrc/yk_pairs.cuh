@@ -167,6 +167,108 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
     }
 }
 
+// ---- which source groups can reach a warp's targets ----------------------
+// The bounding box of a warp's active targets (FP32 copies), computed once per
+// job; a source farther than the screening radius from the box (in the
+// minimum image, with a margin that covers the rounding of the FP32 copies)
+// interacts with none of the 32 targets.  near_groups() classifies a tile's
+// 128 sources against the box, one source per lane at a time, and returns a
+// 32-bit mask of the 4-source groups that have at least one source within
+// reach; the other groups skip even the per-pair FP32 screen.
+struct WarpBox {
+    float lo[3], hi[3];
+    bool any, has_p;                 // any active target; any proton target (nucleons)
+};
+
+__device__ __forceinline__ float warp_minf(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_maxf(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ WarpBox warp_box(const double4& pi, bool active)
+{
+    WarpBox b;
+    const float inf = __int_as_float(0x7f800000);
+    const double c[3] = {pi.x, pi.y, pi.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float v = __double2float_rn(c[k]);
+        b.lo[k] = warp_minf(active ? v : inf);
+        b.hi[k] = warp_maxf(active ? v : -inf);
+    }
+    b.any = __any_sync(0xffffffffu, active);
+    b.has_p = __any_sync(0xffffffffu, active && pi.w == 1.0);
+    return b;
+}
+
+// Lower bound of the minimum-image distance^2 from source (x, w) to the box.
+template <int SIM>
+__device__ __forceinline__ bool box_reaches(const ForceArgs& fa, const WarpBox& b, const float (&x)[3], float w)
+{
+    float dist2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float L = fa.Lf[k];
+        const float mu = 3.814697265625e-6f * L;                 // 2^-18 L
+        const float lo = (b.lo[k] - x[k]) - mu;                  // x_i - x_j over the box
+        const float hi = (b.hi[k] - x[k]) + mu;
+        // distance from 0 to [lo, hi] + s L, the smallest over s = -1, 0, 1
+        const float m0 = fmaxf(0.f, fmaxf(lo, -hi));
+        const float m1 = fmaxf(0.f, fmaxf(lo - L, L - hi));
+        const float m2 = fmaxf(0.f, fmaxf(lo + L, -L - hi));
+        const float m = fminf(m0, fminf(m1, m2));
+        dist2 = fmaf(m, m, dist2);
+    }
+    float lim;
+    if constexpr (SIM == SIM_PURE || SIM == SIM_MIX) {
+        lim = fa.scr_c2;
+    } else {
+        const bool pp = b.has_p && w == 1.0f && fa.coulomb_on;
+        lim = pp ? fmaxf(fa.scr_c2, fa.scr_n2) : fa.scr_n2;
+    }
+    return dist2 <= lim;
+}
+
+// Bits 4k..4k+3 of v -> bit k (k = 0..7): which of 8 groups has a set bit.
+__device__ __forceinline__ unsigned any_of_4(unsigned v)
+{
+    v |= v >> 1;
+    v |= v >> 2;
+    v &= 0x11111111u;
+    v = (v | (v >> 3)) & 0x03030303u;
+    v = (v | (v >> 6)) & 0x000f000fu;
+    v = (v | (v >> 12)) & 0xffu;
+    return v;
+}
+
+template <int SIM>
+__device__ __forceinline__ unsigned near_groups(const ForceArgs& fa, const WarpBox& b, const float* __restrict__ tlf,
+                                                int jlim, int jmin)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned gm = 0;
+#pragma unroll
+    for (int blk = 0; blk < PB / 32; ++blk) {
+        const int j = 32 * blk + lane;
+        bool near = false;
+        if (b.any && j < jlim && j >= jmin) {
+            const float x[3] = {tlf[j], tlf[SHADOW_TILE + j], tlf[2 * SHADOW_TILE + j]};
+            near = box_reaches<SIM>(fa, b, x, tlf[3 * SHADOW_TILE + j]);
+        }
+        gm |= any_of_4(__ballot_sync(0xffffffffu, near)) << (8 * blk);
+    }
+    return gm;
+}
+
 // Shared memory of the half-pair kernels.
 struct PairSmem {
     double4 tile[2][PB];                  // FP64 source tiles (TMA)
@@ -252,6 +354,7 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
     const R_t wi = (SIM == SIM_MIX) ? (R_t)pi.w : (R_t)1;   // Z_i of the reaction
     const bool all_active = (R + 1) * PB <= n;
     const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
+    const WarpBox box = warp_box(pi, active);
     TargetAcc<PREC, MEAS> acc;
     acc.zero();
 
@@ -273,14 +376,16 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
 #pragma unroll
         for (int k = lane; k < PB * 3; k += 32) my_acc[k] = 0.0;
         __syncwarp();
+        // on the diagonal tile only sources after the warp's first target count
+        unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, diag ? 32 * warp + 1 : 0);
         if (!diag && jlim == PB && all_active) {
-            for (int j0 = 0; j0 < PB; j0 += 4)
-                pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active, tid, sw,
-                                                   acc, my_acc);
+            for (; gm; gm &= gm - 1)
+                pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
+                                                   active, tid, sw, acc, my_acc);
         } else {
-            for (int j0 = 0; j0 < jlim; j0 += 4)
-                pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, j0, jlim, diag, active, tid, sw,
-                                                  acc, my_acc);
+            for (; gm; gm &= gm - 1)
+                pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
+                                                  active, tid, sw, acc, my_acc);
         }
         // this warp is done with the tile: the last warp reduces and refills
         __threadfence_block();
