@@ -183,7 +183,7 @@ k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ p
         __syncthreads();
         BoxView bx;
         bx.pos = pos + d->S;
-        bx.posf = posf + (size_t)(d->S / SHADOW_TILE) * 4 * SHADOW_TILE;
+        bx.posf = posf + (size_t)(d->S / SHADOW_TILE) * SHADOW_FLOATS;
         bx.Si = Si + d->Si_off;
         bx.Sj = Sj + d->Sj_off;
         bx.n = sfa.n;
@@ -607,7 +607,7 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
                                     b->key_bits);
     const size_t need = sizeof(double) * (size_t)(9 * ntot + A + 2 * ntot + sj + si + 8LL * b->njobs +
                                                   (long long)NKIN * b->nvb) +
-                        sizeof(double4) * stot + sizeof(float) * 4 * stot + sizeof(int) * (3 * ntot + 2 * stot) +
+                        sizeof(double4) * stot + sizeof(float) * 7 * stot + sizeof(int) * (3 * ntot + 2 * stot) +
                         sizeof(unsigned long long) * 2 * ntot + cub_bytes + sizeof(RepDesc) * nrep +
                         sizeof(int4) * b->njobs + (64u << 20);
     size_t free_b = 0, total_b = 0;
@@ -632,7 +632,7 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
     BALLOC(b->aii, ntot);
     BALLOC(b->rep_of, ntot);
     BALLOC(b->pos, stot);
-    BALLOC(b->posf, 4 * stot);
+    BALLOC(b->posf, (size_t)SHADOW_FLOATS / SHADOW_TILE * stot);      // stot is a multiple of SHADOW_TILE
     BALLOC(b->perm, stot);
     BALLOC(b->iperm, ntot);
     BALLOC(b->keys0, ntot);
@@ -681,7 +681,7 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
     cudaMemcpyAsync(b->aii, ha.data(), sizeof(double) * ntot, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(b->rep_of, hrep.data(), sizeof(int) * ntot, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(b->pos, 0, sizeof(double4) * stot, st);
-    cudaMemsetAsync(b->posf, 0, sizeof(float) * 4 * stot, st);
+    cudaMemsetAsync(b->posf, 0, sizeof(float) * SHADOW_FLOATS / SHADOW_TILE * stot, st);
     cudaMemsetAsync(b->perm, 0xff, sizeof(int) * stot, st);
     cudaMemcpyAsync(b->rd, rd.data(), sizeof(RepDesc) * nrep, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(b->jobs, sorted.data(), sizeof(int4) * sorted.size(), cudaMemcpyHostToDevice, st);

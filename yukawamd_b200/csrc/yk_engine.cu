@@ -222,6 +222,14 @@ static void setup_args(yk_ctx* c)
         }
         f.scr_c2 = (p.sim_type == YK_SIM_NUCLEON && !p.coulomb_on) ? -1.0f : widen2(p.rccut);
         f.scr_n2 = (p.sim_type == YK_SIM_NUCLEON && p.nuclear_on) ? widen2(p.rncut) : -1.0f;
+        // If every screened pair is closer than L/2 by a clear margin, the
+        // image integers of the FP32 screen equal the reference's minimum-image
+        // decision for every pair that interacts (a wrong image would put the
+        // pair beyond L/2, outside every cutoff), and the pair kernel may use
+        // them instead of the exact comparisons.
+        const double Lmin = std::min(p.xl[0], std::min(p.xl[1], p.xl[2]));
+        const double rscr = std::sqrt(std::max((double)f.scr_c2, (double)f.scr_n2));
+        f.img_k = (std::isfinite(rscr) && rscr + std::ldexp(Lmax, -14) < 0.5 * Lmin) ? 1 : 0;
     }
     f.n = c->n;
     f.nuclear_on = p.nuclear_on;
@@ -755,7 +763,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned*)nullptr, (unsigned*)nullptr,
                                     (int*)nullptr, (int*)nullptr, n, 0, 30);
     size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
-                   (sizeof(double4) + sizeof(float4)) * ((size_t)n + SHADOW_TILE) + sizeof(int) * 5 * (size_t)n + cub_bytes +
+                   (sizeof(double4) + sizeof(float) * SHADOW_FLOATS / SHADOW_TILE) * ((size_t)n + SHADOW_TILE) + sizeof(int) * 5 * (size_t)n + cub_bytes +
                    sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;
     const bool pairs_fit = pair_scratch_bytes(n, c->seg) <= PAIR_SCRATCH_BUDGET;
     if (pairs_fit) bytes += pair_scratch_bytes(n, c->seg);
@@ -783,7 +791,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     ALLOC(c->zii, n);
     ALLOC(c->aii, n);
     ALLOC(c->pos, n);
-    ALLOC(c->posf, (size_t)4 * SHADOW_TILE * ((n + SHADOW_TILE - 1) / SHADOW_TILE));
+    ALLOC(c->posf, (size_t)SHADOW_FLOATS * ((n + SHADOW_TILE - 1) / SHADOW_TILE));
     ALLOC(c->perm, n);
     ALLOC(c->iperm, n);
     ALLOC(c->keys0, n);
@@ -837,7 +845,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
         for (int i = 0; i < n; ++i) fill[i] = p->ai > 0.0 ? p->ai : 1.0;
         cudaMemcpyAsync(c->aii, fill.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
     }
-    cudaMemsetAsync(c->posf, 0, sizeof(float) * 4 * SHADOW_TILE * ((n + SHADOW_TILE - 1) / SHADOW_TILE), st);
+    cudaMemsetAsync(c->posf, 0, sizeof(float) * SHADOW_FLOATS * ((n + SHADOW_TILE - 1) / SHADOW_TILE), st);
     cudaMemsetAsync(c->ds, 0, sizeof(DevScalars), st);
     cudaMemsetAsync(c->err, 0, sizeof(unsigned), st);
     cudaMemsetAsync(c->series_idx, 0, sizeof(int), st);
@@ -1331,7 +1339,7 @@ static NoallocLayout noalloc_layout(int n)
         return at;
     };
     L.pos = take(sizeof(double4) * (size_t)n);
-    L.posf = take(sizeof(float) * 4 * SHADOW_TILE * (size_t)L.M);
+    L.posf = take(sizeof(float) * SHADOW_FLOATS * (size_t)L.M);
     L.perm = take(sizeof(int) * (size_t)n);
     L.iperm = take(sizeof(int) * (size_t)n);
     L.Si = take(sizeof(double) * 3 * PB * (size_t)L.M * L.nseg);
@@ -1438,7 +1446,7 @@ extern "C" int yk_accel_noalloc(const yk_params* p, int n, const double* x_dev, 
     const bool meas = do_meas != 0;
 
     // clear what must start at zero: shadow padding, scalars, counter, error word
-    CK(nullptr, cudaMemsetAsync(posf, 0, sizeof(float) * 4 * SHADOW_TILE * (size_t)L.M, st));
+    CK(nullptr, cudaMemsetAsync(posf, 0, sizeof(float) * SHADOW_FLOATS * (size_t)L.M, st));
     CK(nullptr, cudaMemsetAsync(ds, 0, sizeof(DevScalars), st));
     CK(nullptr, cudaMemsetAsync(counter, 0, sizeof(int), st));
     CK(nullptr, cudaMemsetAsync(err, 0, sizeof(unsigned), st));

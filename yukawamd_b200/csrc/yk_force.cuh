@@ -58,16 +58,43 @@ struct ForceArgs {
     float Lf[3], invLf[3];
     float scr_c2, scr_n2;
     int n, nuclear_on, coulomb_on, mix_compat;
+    int img_k;                       // the screen's image integers are exact (see setup)
 };
 
-// FP32 shadow positions ("posf") are stored tile by tile in SoA form: tile t
-// (slots 128t .. 128t+127) is a contiguous block of 512 floats x[128], y[128],
-// z[128], w[128], so a source tile is one 2 KB bulk copy and two neighbouring
-// sources' x (y, z) form one aligned float2.
+// FP32 shadow positions ("posf") are stored tile by tile: tile t (slots
+// 128t .. 128t+127) is a contiguous block of SHADOW_FLOATS = 896 floats, one
+// 256-float section per coordinate and then w[128].  Within a coordinate's
+// section each group of 4 slots s0..s3 takes 8 floats in the order
+//     s0 s1 s1 s0 s2 s3 s3 s2
+// so that (a) two neighbouring slots (j, j+1), j even, are one aligned
+// float2 at offset 2j, and (b) every ordered pair of a group's halves that
+// the half-pair kernel's lane swizzle needs -- (s0,s1) (s1,s0) (s2,s3)
+// (s3,s2) -- is one aligned float2 at offset 2q, q = 0..3, in the block.
+// A source tile is one 3.5 KB bulk copy.
 constexpr int SHADOW_TILE = 128;
-__host__ __device__ __forceinline__ int shadow_index(int slot, int comp)
+constexpr int SHADOW_FLOATS = 7 * SHADOW_TILE;
+__host__ __device__ __forceinline__ int shadow_off(int j, int comp)
 {
-    return (slot >> 7) * (4 * SHADOW_TILE) + comp * SHADOW_TILE + (slot & (SHADOW_TILE - 1));
+    return comp < 3 ? comp * 2 * SHADOW_TILE + 8 * (j >> 2) + ((j & 1) | ((j & 2) << 1))
+                    : 6 * SHADOW_TILE + j;
+}
+// index of slot's (first) copy of component comp; the second copy of
+// comp < 3 is at shadow_index ^ 3
+__host__ __device__ __forceinline__ long long shadow_index(int slot, int comp)
+{
+    return (long long)(slot >> 7) * SHADOW_FLOATS + shadow_off(slot & (SHADOW_TILE - 1), comp);
+}
+
+__device__ __forceinline__ void store_shadow(float* __restrict__ posf, int slot, float x, float y, float z, float w)
+{
+    const float v[3] = {x, y, z};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const long long k = shadow_index(slot, c);
+        posf[k] = v[c];
+        posf[k ^ 3] = v[c];
+    }
+    posf[shadow_index(slot, 3)] = w;
 }
 
 // Target-side constants of the FP32 screen (negated shadow position).
@@ -98,7 +125,7 @@ __device__ __forceinline__ float2 screen_r2_x2(const ForceArgs& fa, const Screen
     const float ni[3] = {si.nx, si.ny, si.nz};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float2 xj = *reinterpret_cast<const float2*>(t + c * SHADOW_TILE + j);
+        const float2 xj = *reinterpret_cast<const float2*>(t + c * 2 * SHADOW_TILE + 2 * j);
         float2 dc = __fadd2_rn(xj, make_float2(ni[c], ni[c]));
         const float2 k = __fadd2_rn(__ffma2_rn(dc, make_float2(fa.invLf[c], fa.invLf[c]), MAG), NMAG);
         d[c] = __ffma2_rn(make_float2(-fa.Lf[c], -fa.Lf[c]), k, dc);
@@ -113,11 +140,33 @@ __device__ __forceinline__ float screen_r2_1(const ForceArgs& fa, const ScreenI&
                                             const float* __restrict__ t, int j)
 {
     const float MAGIC = 12582912.0f;
-    float dx = t[j] + si.nx, dy = t[SHADOW_TILE + j] + si.ny, dz = t[2 * SHADOW_TILE + j] + si.nz;
+    float dx = t[shadow_off(j, 0)] + si.nx, dy = t[shadow_off(j, 1)] + si.ny, dz = t[shadow_off(j, 2)] + si.nz;
     dx = fmaf(-fa.Lf[0], fmaf(dx, fa.invLf[0], MAGIC) - MAGIC, dx);
     dy = fmaf(-fa.Lf[1], fmaf(dy, fa.invLf[1], MAGIC) - MAGIC, dy);
     dz = fmaf(-fa.Lf[2], fmaf(dz, fa.invLf[2], MAGIC) - MAGIC, dz);
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+// The packed screen for the ordered source pair stored at offset off (0, 2,
+// 4 or 6) of group g's blocks, also returning the image integers
+// k = rint(d/L) per axis (as floats: -1, 0 or 1 for a pair in the box).
+__device__ __forceinline__ float2 screen_r2k_x2(const ForceArgs& fa, const ScreenI& si,
+                                                const float* __restrict__ t, int g, int off, float2 (&k)[3])
+{
+    const float2 MAG = make_float2(12582912.0f, 12582912.0f);
+    const float2 NMAG = make_float2(-12582912.0f, -12582912.0f);
+    float2 d[3];
+    const float ni[3] = {si.nx, si.ny, si.nz};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float2 xj = *reinterpret_cast<const float2*>(t + c * 2 * SHADOW_TILE + 8 * g + off);
+        float2 dc = __fadd2_rn(xj, make_float2(ni[c], ni[c]));
+        k[c] = __fadd2_rn(__ffma2_rn(dc, make_float2(fa.invLf[c], fa.invLf[c]), MAG), NMAG);
+        d[c] = __ffma2_rn(make_float2(-fa.Lf[c], -fa.Lf[c]), k[c], dc);
+    }
+    float2 r2 = __fmul2_rn(d[2], d[2]);
+    r2 = __ffma2_rn(d[1], d[1], r2);
+    return __ffma2_rn(d[0], d[0], r2);
 }
 
 // Squared screening radius of a pair.  Ions: rccut.  Nucleons: rncut for the
@@ -269,25 +318,29 @@ __device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, c
 // The screened-Coulomb terms of phys64 / phys32 for a pair that sel says the
 // screen selected; computed unconditionally (a placeholder r^2 = 1 for pairs
 // that do not interact) and masked, so that several pairs' chains can be
-// interleaved by the compiler.  The FP64 form takes the reference's minimum
-// image on integer compares; the mixed form takes it on FP64 compares, which
-// keep it off the integer pipe that the mixed path already loads.
-__device__ __forceinline__ double min_image_cmp(double d, double L, double hL)
+// interleaved by the compiler.
+
+// d = x_i - x_j in the minimum image.  The screen rounds (x_j - x_i)/L to
+// the image integer k, so the reference's d - L (d > L/2) or d + L
+// (d < -L/2) is d + k L, one FMA, when k is exact (fa.img_k, see the host
+// setup); otherwise the conditional corrections themselves.
+__device__ __forceinline__ double image_k(const ForceArgs& fa, double d, float k, int c)
 {
-    double s = 0.0;
-    if (d > hL) s = -L;
-    else if (d < -hL) s = L;
-    return __dadd_rn(d, s);
+    return fa.img_k ? __fma_rn((double)k, fa.xl[c], d) : min_image(d, fa.xl[c], fa.hlb[c]);
 }
 
 template <int PREC, bool MEAS>
 __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& pi, const double4& pj, bool sel,
+                                            const float (&k)[3],
                                             PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o)
 {
+    const double dx = image_k(fa, __dsub_rn(pi.x, pj.x), k[0], 0);
+    const double dy = image_k(fa, __dsub_rn(pi.y, pj.y), k[1], 1);
+    const double dz = image_k(fa, __dsub_rn(pi.z, pj.z), k[2], 2);
     if constexpr (PREC == PREC_FP64) {
-        o.dx = min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]);
-        o.dy = min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]);
-        o.dz = min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]);
+        o.dx = dx;
+        o.dy = dy;
+        o.dz = dz;
         const double r2 = o.dx * o.dx + o.dy * o.dy + o.dz * o.dz;
         const bool hit = sel && r2 <= fa.rc2;
         const double r2s = hit ? r2 : 1.0;
@@ -301,10 +354,9 @@ __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& 
         o.w = (MEAS && hit) ? fs * r2 : 0.0;
         o.hit = hit;
     } else {
-        const double hx = 0.5 * fa.xl[0], hy = 0.5 * fa.xl[1], hz = 0.5 * fa.xl[2];
-        o.dx = __double2float_rn(min_image_cmp(__dsub_rn(pi.x, pj.x), fa.xl[0], hx));
-        o.dy = __double2float_rn(min_image_cmp(__dsub_rn(pi.y, pj.y), fa.xl[1], hy));
-        o.dz = __double2float_rn(min_image_cmp(__dsub_rn(pi.z, pj.z), fa.xl[2], hz));
+        o.dx = __double2float_rn(dx);
+        o.dy = __double2float_rn(dy);
+        o.dz = __double2float_rn(dz);
         const float r2 = fmaf(o.dx, o.dx, fmaf(o.dy, o.dy, o.dz * o.dz));
         const bool hit = sel && r2 <= fa.rc2f;
         const float r2s = hit ? r2 : 1.0f;
@@ -479,7 +531,7 @@ __device__ __forceinline__ void store_accel(const ForceArgs& fa, int orig, doubl
 
 // Shared memory of k_force_rows: 2 stages of FTILE double4 and one shadow tile,
 // 2 mbarriers and the block-reduction scratch.
-constexpr int FORCE_SMEM = 2 * FTILE * (int)(sizeof(double4) + 4 * sizeof(float)) + 16 +
+constexpr int FORCE_SMEM = 2 * FTILE * (int)sizeof(double4) + 2 * SHADOW_FLOATS * (int)sizeof(float) + 16 +
                            32 * NSCAL * (int)sizeof(double);
 
 template <int SIM, int PREC, bool MEAS>
@@ -491,8 +543,8 @@ k_force_rows(const double4* __restrict__ pos, const float* __restrict__ posf,
     extern __shared__ __align__(128) unsigned char smem[];
     double4* tile = reinterpret_cast<double4*>(smem);
     float* tilef = reinterpret_cast<float*>(smem + 2 * FTILE * sizeof(double4));
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * FTILE * (sizeof(double4) + 4 * sizeof(float)));
-    double* red = reinterpret_cast<double*>(smem + 2 * FTILE * (sizeof(double4) + 4 * sizeof(float)) + 16);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * FTILE * sizeof(double4) + 2 * SHADOW_FLOATS * sizeof(float));
+    double* red = reinterpret_cast<double*>(smem + 2 * FTILE * sizeof(double4) + 2 * SHADOW_FLOATS * sizeof(float) + 16);
 
     const int n = fa.n;
     const int i = blockIdx.x * FBLOCK + threadIdx.x;
@@ -511,11 +563,11 @@ k_force_rows(const double4* __restrict__ pos, const float* __restrict__ posf,
         const int j0 = t * FTILE;
         const int cnt = min(FTILE, n - j0);
         const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
-        const unsigned bytesf = 4u * SHADOW_TILE * (unsigned)sizeof(float);
+        const unsigned bytesf = (unsigned)SHADOW_FLOATS * (unsigned)sizeof(float);
         uint64_t* b = &bar[t & 1];
         mbar_arrive_expect_tx(b, bytes + bytesf);
         bulk_g2s(tile + (t & 1) * FTILE, pos + j0, bytes, b);
-        bulk_g2s(tilef + (t & 1) * 4 * SHADOW_TILE, posf + (size_t)t * 4 * SHADOW_TILE, bytesf, b);
+        bulk_g2s(tilef + (t & 1) * SHADOW_FLOATS, posf + (size_t)t * SHADOW_FLOATS, bytesf, b);
     };
     if (threadIdx.x == 0) {
         issue(0);
@@ -539,12 +591,12 @@ k_force_rows(const double4* __restrict__ pos, const float* __restrict__ posf,
         const int j0 = t * FTILE;
         const int cnt = min(FTILE, n - j0);
         const double4* tl = tile + st * FTILE;
-        const float* tlf = tilef + st * 4 * SHADOW_TILE;
+        const float* tlf = tilef + st * SHADOW_FLOATS;
         if (active) {
 #pragma unroll 2
             for (int jj = 0; jj < cnt; ++jj) {
                 if ((j0 + jj) != i &&
-                    screen_r2_1(fa, si, tlf, jj) <= screen_lim<SIM>(fa, si.w, tlf[3 * SHADOW_TILE + jj])) {
+                    screen_r2_1(fa, si, tlf, jj) <= screen_lim<SIM>(fa, si.w, tlf[shadow_off(jj, 3)])) {
                     const double4 pj = tl[jj];
                     pair_eval<SIM, PREC, MEAS>(fa, pi, pj, true, o);
                     if (o.hit) acc.add(o, SIM == SIM_MIX ? (real_t<PREC>)pj.w : (real_t<PREC>)1);

@@ -81,9 +81,13 @@ __device__ __forceinline__ void reduce_scatter4(T (&r)[4][3], T (&t)[3])
         for (int c = 0; c < 3; ++c) t[c] += __shfl_xor_sync(0xffffffffu, t[c], m);
 }
 
-// One group of 4 sources j0..j0+3 for the calling lane's target.  CHECK:
-// the tile is partial, diagonal, or the CTA has inactive targets, so every
-// pair needs the validity test.
+// One group of 4 sources j0..j0+3 for the calling lane's target, taken in
+// the lane's swizzled order: step jj handles source j0 + (jj ^ sw).  The
+// screen runs in the same order from the paired shadow layout (steps 0, 1
+// are the ordered pair at offset 2 sw of the group's blocks, steps 2, 3 the
+// one at 2 (sw ^ 2)), so each step's image integers are plain registers.
+// CHECK: the tile is partial, diagonal, or the CTA has inactive targets, so
+// every pair needs the validity test.
 template <int SIM, int PREC, bool MEAS, bool CHECK>
 __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& pi, const ScreenI& si,
                                            real_t<PREC> wi, const double4* tl, const float* tlf,
@@ -91,20 +95,21 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
                                            int sw, TargetAcc<PREC, MEAS>& acc, double* my_acc)
 {
     using R_t = real_t<PREC>;
-    // screen the 4 sources in natural order, two per packed instruction
-    const float2 ra = screen_r2_x2(fa, si, tlf, j0);
-    const float2 rb = screen_r2_x2(fa, si, tlf, j0 + 2);
-    const float* tw = tlf + 3 * SHADOW_TILE + j0;
-    unsigned m = (ra.x <= screen_lim<SIM>(fa, si.w, tw[0]) ? 1u : 0u) |
-                 (ra.y <= screen_lim<SIM>(fa, si.w, tw[1]) ? 2u : 0u) |
-                 (rb.x <= screen_lim<SIM>(fa, si.w, tw[2]) ? 4u : 0u) |
-                 (rb.y <= screen_lim<SIM>(fa, si.w, tw[3]) ? 8u : 0u);
+    const int g = j0 >> 2;
+    float2 ka[3], kb[3];
+    const float2 ra = screen_r2k_x2(fa, si, tlf, g, 2 * sw, ka);
+    const float2 rb = screen_r2k_x2(fa, si, tlf, g, 2 * (sw ^ 2), kb);
+    const float* tw = tlf + 6 * SHADOW_TILE + j0;
+    unsigned m = (ra.x <= screen_lim<SIM>(fa, si.w, tw[sw]) ? 1u : 0u) |
+                 (ra.y <= screen_lim<SIM>(fa, si.w, tw[sw ^ 1]) ? 2u : 0u) |
+                 (rb.x <= screen_lim<SIM>(fa, si.w, tw[sw ^ 2]) ? 4u : 0u) |
+                 (rb.y <= screen_lim<SIM>(fa, si.w, tw[sw ^ 3]) ? 8u : 0u);
     if constexpr (CHECK) {
         unsigned ok = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int jl = j0 + q;
-            if (active && jl < jlim && (!diag || jl > tid)) ok |= 1u << q;
+        for (int jj = 0; jj < 4; ++jj) {
+            const int jl = j0 + (jj ^ sw);
+            if (active && jl < jlim && (!diag || jl > tid)) ok |= 1u << jj;
         }
         m &= ok;
     }
@@ -119,10 +124,12 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
         // not select, or outside r_c, gets zero terms.
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
-            const int src = jj ^ sw;
-            const double4 pjv = tl[j0 + src];
+            const double4 pjv = tl[j0 + (jj ^ sw)];
+            const float k[3] = {jj == 0 ? ka[0].x : jj == 1 ? ka[0].y : jj == 2 ? kb[0].x : kb[0].y,
+                                jj == 0 ? ka[1].x : jj == 1 ? ka[1].y : jj == 2 ? kb[1].x : kb[1].y,
+                                jj == 0 ? ka[2].x : jj == 1 ? ka[2].y : jj == 2 ? kb[2].x : kb[2].y};
             PairOut<R_t> o;
-            ion_pair_nb<PREC, MEAS>(fa, pi, pjv, ((m >> src) & 1u) != 0, o);
+            ion_pair_nb<PREC, MEAS>(fa, pi, pjv, ((m >> jj) & 1u) != 0, k, o);
             if constexpr (PREC == PREC_FP64) acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
             else gs.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
             const R_t fsj = o.fs * wi;               // 0 unless the pair interacts
@@ -133,28 +140,28 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
         }
     } else {
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-        const int src = jj ^ sw;
-        r[jj][0] = r[jj][1] = r[jj][2] = (R_t)0;
-        if ((m >> src) & 1u) {
-            const double4 pjv = tl[j0 + src];
-            PairOut<R_t> o;
-            pair_eval<SIM, PREC, MEAS>(fa, pi, pjv, true, o);
-            if (o.hit) {
-                if constexpr (PREC == PREC_FP64) acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
-                else gs.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
-                // reaction on j: Z_i fs d (int_ion_mix.f:180)
-                const R_t fsj = o.fs * wi;
-                r[jj][0] = fsj * o.dx;
-                r[jj][1] = fsj * o.dy;
-                r[jj][2] = fsj * o.dz;
-                any = true;
+        for (int jj = 0; jj < 4; ++jj) {
+            r[jj][0] = r[jj][1] = r[jj][2] = (R_t)0;
+            if ((m >> jj) & 1u) {
+                const double4 pjv = tl[j0 + (jj ^ sw)];
+                PairOut<R_t> o;
+                pair_eval<SIM, PREC, MEAS>(fa, pi, pjv, true, o);
+                if (o.hit) {
+                    if constexpr (PREC == PREC_FP64) acc.add(o, (R_t)1);
+                    else gs.add(o, (R_t)1);
+                    const R_t fsj = o.fs * wi;
+                    r[jj][0] = fsj * o.dx;
+                    r[jj][1] = fsj * o.dy;
+                    r[jj][2] = fsj * o.dz;
+                    any = true;
+                }
             }
         }
     }
-    }
     if constexpr (PREC == PREC_MIXED) acc.add_group(gs);
     if (__any_sync(0xffffffffu, any)) {
+        // reaction on j: Z_i fs d (int_ion_mix.f:180); slot jj of lane L
+        // belongs to source jj ^ sw(L), as reduce_scatter4 expects
         R_t t[3];
         reduce_scatter4(r, t);
         const int lane = threadIdx.x & 31;
@@ -261,8 +268,8 @@ __device__ __forceinline__ unsigned near_groups(const ForceArgs& fa, const WarpB
         const int j = 32 * blk + lane;
         bool near = false;
         if (b.any && j < jlim && j >= jmin) {
-            const float x[3] = {tlf[j], tlf[SHADOW_TILE + j], tlf[2 * SHADOW_TILE + j]};
-            near = box_reaches<SIM>(fa, b, x, tlf[3 * SHADOW_TILE + j]);
+            const float x[3] = {tlf[shadow_off(j, 0)], tlf[shadow_off(j, 1)], tlf[shadow_off(j, 2)]};
+            near = box_reaches<SIM>(fa, b, x, tlf[shadow_off(j, 3)]);
         }
         gm |= any_of_4(__ballot_sync(0xffffffffu, near)) << (8 * blk);
     }
@@ -272,7 +279,7 @@ __device__ __forceinline__ unsigned near_groups(const ForceArgs& fa, const WarpB
 // Shared memory of the half-pair kernels.
 struct PairSmem {
     double4 tile[2][PB];                  // FP64 source tiles (TMA)
-    float tilef[2][4 * SHADOW_TILE];      // FP32 shadow source tiles (TMA)
+    float tilef[2][SHADOW_FLOATS];        // FP32 shadow source tiles (TMA)
     double acc_j[2][PWARPS][PB * 3];      // per-warp reaction rows, one set per tile stage
     double red[32 * NSCAL];               // block reduction scratch
     uint64_t bar[2];                      // one mbarrier per tile stage
@@ -298,7 +305,7 @@ __device__ __forceinline__ void pairs_smem_init(PairSmem& sm)
     // filled.  Zero them once: from then on every slot holds a finite position
     // (zero, or one left by an earlier tile) and a masked pair yields 0, not NaN.
     for (int k = threadIdx.x; k < 2 * PB; k += blockDim.x) (&sm.tile[0][0])[k] = make_double4(0.0, 0.0, 0.0, 0.0);
-    for (int k = threadIdx.x; k < 2 * 4 * SHADOW_TILE; k += blockDim.x) (&sm.tilef[0][0])[k] = 0.f;
+    for (int k = threadIdx.x; k < 2 * SHADOW_FLOATS; k += blockDim.x) (&sm.tilef[0][0])[k] = 0.f;
     if (threadIdx.x == 0) {
         mbar_init(&sm.bar[0], 1);
         mbar_init(&sm.bar[1], 1);
@@ -315,11 +322,11 @@ __device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int
     const int j0 = C * PB;
     const int cnt = min(PB, bx.n - j0);
     const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
-    const unsigned bytesf = 4u * SHADOW_TILE * (unsigned)sizeof(float);
+    const unsigned bytesf = (unsigned)SHADOW_FLOATS * (unsigned)sizeof(float);
     uint64_t* b = &sm.bar[qq & 1];
     mbar_arrive_expect_tx(b, bytes + bytesf);
     bulk_g2s(&sm.tile[qq & 1][0], bx.pos + j0, bytes, b);
-    bulk_g2s(&sm.tilef[qq & 1][0], bx.posf + (size_t)C * 4 * SHADOW_TILE, bytesf, b);
+    bulk_g2s(&sm.tilef[qq & 1][0], bx.posf + (size_t)C * SHADOW_FLOATS, bytesf, b);
 }
 
 // Job (R, sg) of box bx: target block R against source tiles

@@ -42,7 +42,7 @@ def footprint_bytes(n, seg=8):
     t = (n + PB - 1) // PB
     nseg = (t + seg - 1) // seg
     scratch = 8 * 3 * PB * (t * (t + 1) // 2 + t * nseg)
-    return 260 * n + 48 * PB * t + scratch + 4096
+    return 260 * n + 60 * PB * t + scratch + 4096
 
 
 @dataclass
