@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--ensemble-steps", type=int, default=100)
     ap.add_argument("--serve", action="store_true",
                     help="instead of the benchmark: serve a request stream and report latency")
+    ap.add_argument("--serve-ensemble", action="store_true",
+                    help="instead of the benchmark: serve the 256-replica ensemble and report latency")
+    ap.add_argument("--ensemble-serve-steps", type=int, default=1000)
     ap.add_argument("--serve-count", type=int, default=48)
     ap.add_argument("--serve-rate", type=float, default=8.0)
     ap.add_argument("--serve-nmax", type=int, default=32768)
@@ -106,47 +109,68 @@ def workload_desc(w, kind):
 # distributed plumbing (torch.distributed for barriers and the max over ranks)
 
 class Dist:
+    """One process per GPU (torchrun env vars).  NCCL on GPUs; gloo when no GPU
+    is visible (the CPU tests of this plumbing).  Every rank makes the same
+    collective calls in the same order; the process group has a short timeout
+    so that a rank that never arrives ends the others' next collective with
+    an error instead of a hang."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = False
         self.torch = None
+        self.dev = "cpu"
 
-    def init(self):
+    def init(self, backend=None, timeout_s=120):
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.dev = "cuda"
+                kw["device_id"] = torch.device("cuda", self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
             self.torch = torch
             self.pg = True
 
     def barrier(self):
         if self.pg:
-            t = self.torch.ones(1, device="cuda")
+            t = self.torch.ones(1, device=self.dev)
             self.torch.distributed.all_reduce(t)
-            self.torch.cuda.synchronize()
+            if self.dev == "cuda":
+                self.torch.cuda.synchronize()
+
+    def _reduce(self, x, op):
+        t = self.torch.tensor([float(x)], device=self.dev, dtype=self.torch.float64)
+        self.torch.distributed.all_reduce(t, op=op)
+        return float(t.item())
 
     def max(self, x):
         if not self.pg:
             return x
-        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
-        self.torch.distributed.all_reduce(t, op=self.torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return self._reduce(x, self.torch.distributed.ReduceOp.MAX)
 
     def sum(self, x):
         if not self.pg:
             return x
-        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
-        self.torch.distributed.all_reduce(t)
-        return float(t.item())
+        return self._reduce(x, self.torch.distributed.ReduceOp.SUM)
 
     def close(self):
         if self.pg:
             self.torch.distributed.destroy_process_group()
+            self.pg = False
+
+
+def job_rate(world, units_per_rank, ms_max):
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank units, timed as the slowest rank (ms)."""
+    return world * units_per_rank / (ms_max * 1e-3)
 
 
 # ---------------------------------------------------------------------------
@@ -343,7 +367,7 @@ def run_ours(args, dist):
     clk = clocks.stop()
     ms_local = perf.run_ms
     ms = dist.max(ms_local)
-    value = dist.world * pairs_step * K / (ms * 1e-3)
+    value = job_rate(dist.world, pairs_step * K, ms)
 
     # dominant kernel: the force kernel, timed live with events on its stream
     force_ms = perf.force_ms / max(perf.force_calls, 1)
@@ -380,7 +404,7 @@ def run_ours(args, dist):
         other = "mixed" if args.precision == "fp64" else "fp64"
         e2, perf2, _ = time_engine(w, other, K, W, me, dist)
         ms2 = dist.max(perf2.run_ms)
-        v2 = dist.world * pairs_step * K / (ms2 * 1e-3)
+        v2 = job_rate(dist.world, pairs_step * K, ms2)
         # force accuracy of the mixed form against FP64 on the same positions
         from yukawamd_b200 import abi
         from yukawamd_b200.engine import Engine
@@ -516,6 +540,34 @@ def serve_stream(args, dist):
     return rep
 
 
+def serve_ensemble(args, dist):
+    """The 256-replica ensemble served: every replica is a request of
+    args.ensemble_serve_steps steps submitted at t = 0; the server keeps them
+    resident and advances them as one batch (one persistent force kernel per
+    step, CUDA graphs of 50 steps) with the job segment length the autotuner
+    picked on this ensemble.  Reports p50 / p99 completion latency and the
+    aggregate pair-interactions/s."""
+    from yukawamd_b200 import abi, configs, tune
+    from yukawamd_b200.engine import Batch
+    from yukawamd_b200.serve import Request, Server
+    boxes = configs.replica_ensemble(args.seed + 2 + 1000 * dist.rank)
+    t0 = time.perf_counter()
+    with Batch(boxes, device=dist.local, precision=abi.YK_PREC_MIXED) as b:
+        b.accel(True)
+        best, best_ms, tried = tune.tune_batch(b, steps=50, device=dist.local)
+    tune_s = time.perf_counter() - t0
+    reqs = [Request(i, w, args.ensemble_serve_steps, abi.YK_PREC_MIXED, 0.0) for i, w in enumerate(boxes)]
+    rep = Server(device=dist.local, chunk=50, autotune=True).run(reqs)
+    rep.update({"metric": "served 256-replica ensemble: p50 / p99 completion latency; aggregate "
+                          "pair-interactions/s",
+                "ensemble": "256 pure-ion boxes, N log-uniform in [1e3, 2e4], Gamma U[50,250], kappa "
+                            "U[0.5,2], Z in {6,8,26}, seed %d, %d steps each, all submitted at t = 0, "
+                            "mixed precision" % (args.seed + 2 + 1000 * dist.rank, args.ensemble_serve_steps),
+                "autotune": {"pair_seg": best, "graph_ms_50_steps": best_ms,
+                             "tried": [[ms, seg] for ms, seg in tried], "wall_s": tune_s}})
+    return rep
+
+
 def run_reference(args):
     """The reference's CPU algorithm (OpenMP C restatement) on all host cores."""
     from oracle.oracle import Oracle
@@ -575,6 +627,11 @@ def main():
     dist = Dist()
     dist.init()
     try:
+        if args.serve_ensemble:
+            out = serve_ensemble(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(out), flush=True)
+            return 0
         if args.serve:
             out = serve_stream(args, dist)
             if dist.rank == 0:

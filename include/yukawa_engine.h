@@ -243,15 +243,24 @@ YK_API int yk_batch_set_state(yk_batch* b, int rep, const double* x,
  */
 typedef struct yk_tuning {
     int force_kernel;     /* 0 auto, 1 row kernel (each pair from both sides),
-                             2 half-pair kernel (Newton's third law, scratch);
+                             2 half-pair kernel (Newton's third law, scratch),
+                             3 half-pair kernel over per-warp near-source lists;
                              yk_get_tuning reports the kernel auto resolved to */
     int pair_seg;         /* source tiles per job of the half-pair kernel     */
-    int sort_every;       /* steps between Morton re-orderings (-1 = never)   */
+    int sort_every;       /* steps between Hilbert re-orderings (-1 = never)  */
     int graph_steps;      /* steps captured per CUDA graph by yk_run          */
 } yk_tuning;
 
 YK_API int yk_get_tuning(yk_ctx* ctx, yk_tuning* out);
 YK_API int yk_set_tuning(yk_ctx* ctx, const yk_tuning* t);
+
+/* The batch's tunables: pair_seg (source tiles per job, all boxes) and
+ * graph_steps (steps per CUDA graph of yk_batch_run; the batch re-sorts at
+ * the start of every graph, which yk_batch_get_tuning reports as
+ * sort_every).  force_kernel must be 0 or 2.  Changing pair_seg rebuilds
+ * the job table and its scratch. */
+YK_API int yk_batch_get_tuning(yk_batch* b, yk_tuning* out);
+YK_API int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t);
 
 /*
  * Timers, the counterpart of the reference's perf.f report (perf.f:60-178:

@@ -99,3 +99,27 @@ def test_batch_rejects_mixed_kinds(gpu):
     with pytest.raises(EngineError) as ei:
         Batch([ion_boxes()[0], nucleon_boxes()[0]])
     assert ei.value.code == abi.YK_ERR_ARG
+
+
+def test_batch_tuning_changes_nothing_but_speed(gpu):
+    """pair_seg only re-cuts the work items: accelerations agree with the
+    default cut to summation-order rounding, and a graph run after the
+    re-cut continues correctly."""
+    from yukawamd_b200 import tune
+    boxes = ion_boxes()
+    with Batch(boxes, mix_mode=abi.YK_MIX_FIXED) as b:
+        b.accel(True)
+        a0 = [b.get_state(r)[3] for r in range(b.nrep)]
+        assert b.tuning().pair_seg == 8
+        t = b.set_tuning(pair_seg=3, graph_steps=20)
+        assert t.pair_seg == 3 and t.graph_steps == 20
+        b.accel(True)
+        a1 = [b.get_state(r)[3] for r in range(b.nrep)]
+        for r, w in enumerate(boxes):
+            n = w.n
+            if n > 1:
+                assert _rel(a1[r][:3 * n], a0[r][:3 * n]) <= 1e-13
+        best, best_ms, tried = tune.tune_batch(b, segs=(8, 3), steps=20, save=False)
+        assert best in (8, 3) and best_ms > 0 and len(tried) == 2
+        assert b.tuning().pair_seg == best
+        b.run(45, 10, series=False)

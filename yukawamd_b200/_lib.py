@@ -40,6 +40,8 @@ SIGNATURES = {
     "yk_batch_create": (C.c_int, [C.c_int, _P, C.POINTER(C.c_int), C.POINTER(_dp), C.POINTER(_dp),
                                   C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(_ctx)]),
     "yk_batch_destroy": (C.c_int, [_ctx]),
+    "yk_batch_get_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
+    "yk_batch_set_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_batch_last_error": (C.c_char_p, [_ctx]),
     "yk_batch_accel": (C.c_int, [_ctx, C.c_int, _S]),
     "yk_batch_run": (C.c_int, [_ctx, C.c_int, C.c_int, _S, C.POINTER(C.c_double)]),

@@ -51,6 +51,7 @@ struct RepDesc {
     long long A;        // first double of the box's a(3,0:n+2)
     int sm_off;         // first Sm row
     int njobs;
+    int seg;            // source tiles per job
     int kb0, nkb;       // integrator blocks (and kinetic partial rows)
     double raw_scale;   // factor on the packed raw sums: 1/zi^2 for pure-ion
                         // boxes (run as mixtures, their sums carry Z_i Z_j)
@@ -188,7 +189,7 @@ k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ p
         bx.Sj = Sj + d->Sj_off;
         bx.n = sfa.n;
         bx.M = d->T;
-        bx.seg = BATCH_SEG;
+        bx.seg = d->seg;
         bx.nseg_max = d->nseg;
         if (!pairs_job<SIM, PREC, MEAS>(sm, sfa, bx, jb.y, jb.z, Sm + (size_t)(d->sm_off + jb.w) * NSCAL,
                                         err, q))
@@ -208,7 +209,7 @@ k_b_combine(const int* __restrict__ tile_rep, const RepDesc* __restrict__ rd, co
     const int pl = p - d->S;
     if (pl >= d->fa.n) return;
     const int R = pl / PB, l = pl % PB;
-    const int nseg = (d->T - R + BATCH_SEG - 1) / BATCH_SEG;
+    const int nseg = (d->T - R + d->seg - 1) / d->seg;
     double F[3] = {0.0, 0.0, 0.0};
     const double* si = Si + d->Si_off + ((size_t)R * d->nseg * PB + l) * 3;
     for (int s = 0; s < nseg; ++s) {
@@ -291,6 +292,8 @@ struct yk_batch {
     int series_cap = 0;
     int* series_idx = nullptr;
     int force_grid = 0;
+    int seg = BATCH_SEG, graph_steps = BATCH_GRAPH_STEPS;
+    std::vector<RepDesc> hrd;       // host copy of the descriptors
     bool need_sort = true, pos_dirty = false;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::vector<GraphB> graphs;
@@ -460,6 +463,83 @@ extern "C" {
 
 const char* yk_batch_last_error(const yk_batch* b) { return b ? b->errmsg.c_str() : g_batch_err.c_str(); }
 
+// Job table and target-side scratch layout for segment length seg: a job is
+// (box, target block R, segment s) over at most seg source tiles; jobs run
+// costliest first.  Fills the descriptors' seg, nseg, Si_off, sm_off, njobs.
+static void layout_jobs(yk_batch* b, int seg, std::vector<int4>& sorted, long long& si_total)
+{
+    std::vector<int4> jobs;
+    std::vector<int> jcost;
+    long long si = 0;
+    int smo = 0;
+    for (int r = 0; r < b->nrep; ++r) {
+        RepDesc& d = b->hrd[r];
+        const int T = d.T;
+        d.seg = seg;
+        d.nseg = (T + seg - 1) / seg;
+        d.Si_off = si;
+        d.sm_off = smo;
+        int local = 0;
+        for (int R = 0; R < T; ++R)
+            for (int s = 0; s * seg < T - R; ++s) {
+                jobs.push_back(make_int4(r, R, s, local++));
+                const int tiles = std::min(seg, T - R - s * seg);
+                jcost.push_back(2 * tiles - (s == 0 ? 1 : 0));
+            }
+        d.njobs = local;
+        si += (long long)T * d.nseg * PB * 3;
+        smo += local;
+    }
+    std::vector<int> order(jobs.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+    std::stable_sort(order.begin(), order.end(), [&](int u, int w) { return jcost[u] > jcost[w]; });
+    sorted.resize(jobs.size());
+    for (size_t k = 0; k < order.size(); ++k) sorted[k] = jobs[order[k]];
+    b->njobs = (int)sorted.size();
+    b->seg = seg;
+    si_total = si;
+}
+
+int yk_batch_get_tuning(yk_batch* b, yk_tuning* out)
+{
+    if (!b || !out) return bfail(b, YK_ERR_ARG, "batch and out are required");
+    out->force_kernel = 2;
+    out->pair_seg = b->seg;
+    out->sort_every = b->graph_steps;       // the batch re-sorts at the start of every graph
+    out->graph_steps = b->graph_steps;
+    return YK_OK;
+}
+
+int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t)
+{
+    if (!b || !t) return bfail(b, YK_ERR_ARG, "batch and tuning are required");
+    if (t->force_kernel != 0 && t->force_kernel != 2)
+        return bfail(b, YK_ERR_UNSUPPORTED, "a batch runs the half-pair kernel (force_kernel 0 or 2)");
+    if (t->pair_seg < 0 || t->graph_steps < 0) return bfail(b, YK_ERR_ARG, "bad tuning values");
+    BCK(b, cudaSetDevice(b->dev));
+    BCK(b, cudaStreamSynchronize(b->stream));
+    drop_graphs_b(b);
+    b->graph_steps = t->graph_steps > 0 ? t->graph_steps : BATCH_GRAPH_STEPS;
+    const int seg = t->pair_seg > 0 ? t->pair_seg : BATCH_SEG;
+    if (seg == b->seg) return YK_OK;
+    std::vector<int4> sorted;
+    long long si = 0;
+    layout_jobs(b, seg, sorted, si);
+    cudaFree(b->Si);
+    cudaFree(b->Sm);
+    cudaFree(b->jobs);
+    b->Si = b->Sm = nullptr;
+    b->jobs = nullptr;
+    if (cudaMalloc((void**)&b->Si, sizeof(double) * (size_t)std::max<long long>(si, 1)) != cudaSuccess ||
+        cudaMalloc((void**)&b->Sm, sizeof(double) * 8 * (size_t)std::max(b->njobs, 1)) != cudaSuccess ||
+        cudaMalloc((void**)&b->jobs, sizeof(int4) * (size_t)std::max(b->njobs, 1)) != cudaSuccess)
+        return bfail(b, YK_ERR_NOMEM, "re-allocating the job scratch for pair_seg %d failed", seg);
+    BCK(b, cudaMemcpyAsync(b->rd, b->hrd.data(), sizeof(RepDesc) * b->nrep, cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaMemcpyAsync(b->jobs, sorted.data(), sizeof(int4) * sorted.size(), cudaMemcpyHostToDevice,
+                           b->stream));
+    return sync_check_b(b);
+}
+
 int yk_batch_destroy(yk_batch* b)
 {
     if (!b) return bfail(nullptr, YK_ERR_ARG, "batch is NULL");
@@ -530,12 +610,11 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
     b->dt.resize(nrep);
 
     // host-side layout, descriptors, job table, block tables
-    std::vector<RepDesc> rd(nrep);
-    std::vector<int4> jobs;
-    std::vector<int> jcost, tile_rep;
+    b->hrd.resize(nrep);
+    std::vector<RepDesc>& rd = b->hrd;
+    std::vector<int> tile_rep;
     std::vector<int2> vblocks;
     long long P = 0, S = 0, A = 0, sj = 0, si = 0;
-    int smo = 0;
     for (int r = 0; r < nrep; ++r) {
         yk_params p = params[r];
         RepDesc& d = rd[r];
@@ -559,19 +638,8 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
         d.P = (int)P;
         d.S = (int)S;
         d.T = T;
-        d.nseg = (T + BATCH_SEG - 1) / BATCH_SEG;
         d.Sj_off = sj;
-        d.Si_off = si;
         d.A = A;
-        d.sm_off = smo;
-        int local = 0;
-        for (int R = 0; R < T; ++R)
-            for (int s = 0; s * BATCH_SEG < T - R; ++s) {
-                jobs.push_back(make_int4(r, R, s, local++));
-                const int tiles = std::min(BATCH_SEG, T - R - s * BATCH_SEG);
-                jcost.push_back(2 * tiles - (s == 0 ? 1 : 0));
-            }
-        d.njobs = local;
         const int nb = (n[r] + VBLOCK - 1) / VBLOCK;
         d.kb0 = (int)vblocks.size();
         d.nkb = nb;
@@ -586,15 +654,9 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
         S += (long long)T * PB;
         A += 3LL * (n[r] + 3);
         sj += (long long)T * (T + 1) / 2 * PB * 3;
-        si += (long long)T * d.nseg * PB * 3;
-        smo += local;
     }
-    std::vector<int> order(jobs.size());
-    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
-    std::stable_sort(order.begin(), order.end(), [&](int u, int w) { return jcost[u] > jcost[w]; });
-    std::vector<int4> sorted(jobs.size());
-    for (size_t k = 0; k < order.size(); ++k) sorted[k] = jobs[order[k]];
-    b->njobs = (int)sorted.size();
+    std::vector<int4> sorted;
+    layout_jobs(b, BATCH_SEG, sorted, si);
     b->nvb = (int)vblocks.size();
     int bits = 1;
     while ((1 << bits) < nrep) ++bits;
@@ -747,7 +809,7 @@ int yk_batch_run(yk_batch* b, int nsteps, int meas_every, yk_scalars* series, do
     BCK(b, cudaMemsetAsync(b->series_idx, 0, sizeof(int), st));
     BCK(b, cudaEventRecord(b->e0, st));
     const int me = meas_every;
-    const int K = BATCH_GRAPH_STEPS;
+    const int K = b->graph_steps;
     int k = 0, s = 1;
     if (b->pos_dirty || b->need_sort) k += enqueue_sort(b);
     while (s + K - 1 <= nsteps) {

@@ -230,6 +230,20 @@ class Batch:
                                               int(device), C.byref(self._b)))
         self._keep = None
 
+    def tuning(self):
+        t = abi.YkTuning()
+        check_batch(self._lib.yk_batch_get_tuning(self._b, C.byref(t)), self._b)
+        return t
+
+    def set_tuning(self, pair_seg=None, graph_steps=None):
+        t = self.tuning()
+        if pair_seg is not None:
+            t.pair_seg = int(pair_seg)
+        if graph_steps is not None:
+            t.graph_steps = int(graph_steps)
+        check_batch(self._lib.yk_batch_set_tuning(self._b, C.byref(t)), self._b)
+        return self.tuning()
+
     def accel(self, do_measurements=True):
         out = (abi.YkScalars * self.nrep)()
         check_batch(self._lib.yk_batch_accel(self._b, int(bool(do_measurements)), out), self._b)

@@ -93,10 +93,11 @@ def admit(waiting, active_bytes, budget, seg=8):
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget=None, chunk=50, shadow_every=16):
+    def __init__(self, device=0, hbm_budget=None, chunk=50, shadow_every=16, autotune=False):
         self.device = device
         self.chunk = chunk
         self.shadow_every = shadow_every
+        self.autotune = autotune          # apply cached batch tunings (tune.apply_batch)
         if hbm_budget is None:
             import torch
             free, _total = torch.cuda.mem_get_info(device)
@@ -130,6 +131,10 @@ class Server:
                 boxes.append((p, x, v, w.zii, w.aii))
                 fresh.append(False)
         batch = Batch(boxes, device=self.device)
+        if self.autotune:
+            from . import tune
+            tune.apply_batch(batch, self.device)
+        batch.set_tuning(graph_steps=self.chunk)      # one CUDA graph per chunk
         batch.accel(True)                            # md.F:69 for the new runs
         for i, r in enumerate(runs):
             if not fresh[i]:

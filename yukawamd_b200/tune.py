@@ -114,6 +114,48 @@ def tune(engine, candidates=None, steps=6, warmup=2, device=0, save=True):
     return best, best_ms, results
 
 
+BATCH_SEGS = (8, 4, 16, 2, 32)
+
+
+def batch_key(batch, device=0):
+    import numpy as np
+    p = batch.params[0]
+    return "%s|batch|sim%d|prec%d|nrep%d|nb%d" % (gpu_name(device), p.sim_type, p.precision, batch.nrep,
+                                                  bucket(int(np.sqrt(np.mean(np.square(batch.n))))))
+
+
+def tune_batch(batch, segs=BATCH_SEGS, steps=50, device=0, save=True):
+    """Time one graph of `steps` steps of the whole batch for every job
+    segment length (source tiles per work item) and keep the fastest.  The
+    boxes' states are restored afterwards.  Cached per (GPU, sim, precision,
+    box count, RMS box size bucket)."""
+    states = [batch.get_state(r) for r in range(batch.nrep)]
+    results = []
+    for seg in segs:
+        batch.set_tuning(pair_seg=seg, graph_steps=steps)
+        batch.run(steps, 0, series=False)                  # capture + warm
+        _, ms = batch.run(steps, 0, series=False)
+        results.append((ms, seg))
+        for r, (x, v, vold, a) in enumerate(states):
+            batch.set_state(r, x=x, v=v, vold=vold, a=a)
+    best_ms, best = min(results)
+    batch.set_tuning(pair_seg=best, graph_steps=steps)
+    if save:
+        doc = _load()
+        doc[batch_key(batch, device)] = dict(pair_seg=best, graph_steps=steps, ms=best_ms, when=time.time(),
+                                            tried=results)
+        _store(doc)
+    return best, best_ms, results
+
+
+def apply_batch(batch, device=0):
+    ent = _load().get(batch_key(batch, device))
+    if not ent:
+        return False
+    batch.set_tuning(pair_seg=ent["pair_seg"], graph_steps=ent.get("graph_steps", 50))
+    return True
+
+
 def apply(engine, device=0):
     """Apply the cached choice for this engine's bucket; True if one existed."""
     ent = _load().get(key_for(engine, device))
