@@ -342,14 +342,28 @@ def cpu_sample(w, kind, target_s=12.0):
 
     dt, pairs = run(64)                                   # calibration
     rate = pairs / max(dt, 1e-6)
-    nrows = int(min(n // 2 - 1, max(64, target_s * rate / (n - mid))))
-    dt, pairs = run(nrows)
+    total = n * (n - 1) // 2
+    if target_s * rate < total / 2:
+        # less than half a force call: a block of target rows from the middle
+        nrows = int(min(n // 2 - 1, max(64, target_s * rate / (n - mid))))
+        dt, pairs = run(nrows)
+        what = "target rows %d..%d of" % (mid, mid + nrows)
+    else:
+        # whole force calls, repeated to about target_s
+        reps = max(1, int(round(target_s * rate / total)))
+        orc.set_row_range()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            orc.accel(p, w.x, w.zii, w.aii, False)
+        dt = time.perf_counter() - t0
+        pairs = reps * total
+        what = "%d complete force calls over" % reps
     orc.set_row_range()
     return {"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "one force-only call of the oracle's OpenMP loop (int_ion_mix.f "
-                      "structure, OMP_SCHEDULE=%s) over target rows %d..%d of the full N=%d box: "
-                      "%d pairs in %.2f s" % (os.environ.get("OMP_SCHEDULE", "static"), mid,
-                                             mid + nrows, n, pairs, dt)}
+            "sample": "force-only calls of the oracle's OpenMP loop (%s structure, OMP_SCHEDULE=%s): "
+                      "%s the full N=%d box, %d pairs in %.2f s"
+                      % ({"mix": "int_ion_mix.f", "ocp": "int_ion_pure.f"}.get(kind, "int_nn.f"),
+                         os.environ.get("OMP_SCHEDULE", "static"), what, n, pairs, dt)}
 
 
 def run_ours(args, dist):
