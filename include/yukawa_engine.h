@@ -246,7 +246,9 @@ typedef struct yk_tuning {
                              2 half-pair kernel (Newton's third law, scratch),
                              3 half-pair kernel over per-warp near-source lists;
                              yk_get_tuning reports the kernel auto resolved to */
-    int pair_seg;         /* source tiles per job of the half-pair kernel     */
+    int pair_seg;         /* source tiles per job of the half-pair kernels;
+                             0 = automatic (8, shorter for small boxes so that
+                             every resident CTA gets at least two jobs)       */
     int sort_every;       /* steps between Hilbert re-orderings (-1 = never)  */
     int graph_steps;      /* steps captured per CUDA graph by yk_run          */
 } yk_tuning;

@@ -107,6 +107,7 @@ struct yk_ctx {
     int kernel = 2;                 // 1 rows, 2 pairs, 3 near lists (resolved, never 0)
     int kernel_req = 0;             // as requested (0 = auto)
     int seg = DEFAULT_SEG;
+    bool seg_auto = true;           // pair_seg not set by the caller: pick it from N
     int sort_every = DEFAULT_SORT_EVERY;
     int graph_steps = DEFAULT_GRAPH_STEPS;
     long long step_count = 0;       // integrator steps since create
@@ -308,10 +309,27 @@ static void free_pairs(yk_ctx* c)
 
 // Build the job table of the half-pair kernel (costliest jobs first) and its
 // scratch.  Unused Sj / Si slots are never read.
+// Jobs of the half-pair kernels for M tiles cut into runs of seg tiles.
+static long long pair_job_count(int M, int seg)
+{
+    long long k = 0;
+    for (int R = 0; R < M; ++R) k += (M - R + seg - 1) / seg;
+    return k;
+}
+
 static int setup_pairs(yk_ctx* c)
 {
     free_pairs(c);
     const int M = (c->n + PB - 1) / PB;
+    if (c->seg_auto) {
+        // The longest job bounds the force call: keep at least two jobs per
+        // resident CTA (5 per SM), cutting runs shorter for small boxes.
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+        int seg = DEFAULT_SEG;
+        while (seg > 1 && pair_job_count(M, seg) < 2LL * 5 * sms) seg >>= 1;
+        c->seg = seg;
+    }
     const int seg = c->seg;
     std::vector<int2> jobs;
     std::vector<int> cost;
@@ -886,6 +904,7 @@ int yk_set_tuning(yk_ctx* c, const yk_tuning* t)
     CK(c, cudaStreamSynchronize(c->stream));
     drop_graphs(c);
     c->kernel_req = t->force_kernel;
+    c->seg_auto = t->pair_seg <= 0;
     c->seg = t->pair_seg > 0 ? t->pair_seg : DEFAULT_SEG;
     const int old_sort = c->sort_every;
     c->sort_every = t->sort_every == 0 ? DEFAULT_SORT_EVERY : t->sort_every;
