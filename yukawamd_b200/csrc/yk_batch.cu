@@ -59,9 +59,11 @@ struct RepDesc {
 
 // ---- kernels ---------------------------------------------------------------
 
+// Key = (box, [species,] Hilbert index): boxes stay contiguous; in nucleon
+// batches the protons of each box come first (as k_morton).
 __global__ void k_b_morton(const double* __restrict__ x, const int* __restrict__ rep_of,
                            const RepDesc* __restrict__ rd, int ntot, unsigned long long* __restrict__ keys,
-                           int* __restrict__ idx)
+                           int* __restrict__ idx, const double* __restrict__ species)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ntot) return;
@@ -71,7 +73,8 @@ __global__ void k_b_morton(const double* __restrict__ x, const int* __restrict__
     const int cy = min(max((int)(x[3 * i + 1] * (1024.0 / L[1])), 0), 1023);
     const int cz = min(max((int)(x[3 * i + 2] * (1024.0 / L[2])), 0), 1023);
     const unsigned m = hilbert10(cx, cy, cz);
-    keys[i] = ((unsigned long long)r << 30) | m;
+    keys[i] = species ? (((unsigned long long)r << 31) | ((species[i] != 1.0 ? 1ull : 0ull) << 30) | m)
+                      : (((unsigned long long)r << 30) | m);
     idx[i] = i;
 }
 
@@ -326,7 +329,8 @@ static int enqueue_sort(yk_batch* b)
 {
     const int nb = (b->ntot + 255) / 256;
     cudaStream_t st = b->stream;
-    k_b_morton<<<nb, 256, 0, st>>>(b->x, b->rep_of, b->rd, b->ntot, b->keys0, b->idx0);
+    k_b_morton<<<nb, 256, 0, st>>>(b->x, b->rep_of, b->rd, b->ntot, b->keys0, b->idx0,
+                                   b->sim == SIM_NUCLEON ? b->zii : nullptr);
     size_t bytes = b->cub_bytes;
     cub::DeviceRadixSort::SortPairs(b->cub_tmp, bytes, b->keys0, b->keys1, b->idx0, b->idx1, b->ntot, 0,
                                     b->key_bits, st);
@@ -660,7 +664,7 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
     b->nvb = (int)vblocks.size();
     int bits = 1;
     while ((1 << bits) < nrep) ++bits;
-    b->key_bits = 30 + bits;
+    b->key_bits = (nuc ? 31 : 30) + bits;
 
     // admission: refuse up front when the device cannot hold the batch
     size_t cub_bytes = 0;

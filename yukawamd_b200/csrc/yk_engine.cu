@@ -364,14 +364,12 @@ static int setup_pairs(yk_ctx* c)
 static int resolve_kernel(yk_ctx* c)
 {
     int k = c->kernel_req;
-    // Automatic choice: the half-pair kernels while their scratch fits, else
-    // the row kernel.  Ions take the per-pair-screened kernel; nucleons take
-    // the near-list kernel, whose per-(warp, source) image choice pays off
-    // when every proton pair interacts through the p-p Coulomb term (1.5x on
-    // the 51,200-nucleon box; 0.8x on the 55,296-ion mixture).
-    if (k == 0)
-        k = (pair_scratch_bytes(c->n, c->seg) <= PAIR_SCRATCH_BUDGET) ? (c->p.sim_type == YK_SIM_NUCLEON ? 3 : 2)
-                                                                       : 1;
+    // Automatic choice: the per-pair-screened half-pair kernel while its
+    // scratch fits, else the row kernel.  (The near-list kernel, 3, is an
+    // autotuner candidate: with nucleons in species-major slot order it is
+    // 1.35x slower than kernel 2 on the 51,200-nucleon box, and on the
+    // 55,296-ion mixture 1.5x slower.)
+    if (k == 0) k = (pair_scratch_bytes(c->n, c->seg) <= PAIR_SCRATCH_BUDGET) ? 2 : 1;
     if (k == 2 || k == 3) {
         int rc = setup_pairs(c);
         if (rc) return rc;
@@ -406,11 +404,12 @@ static int enqueue_order(yk_ctx* c, bool sort)
             // fixed identity order
             k_morton<<<nb, VBLOCK, 0, st>>>(c->x, n, 0.0, 0.0, 0.0, c->keys0, c->perm);
         } else {
+            const bool nuc = c->p.sim_type == YK_SIM_NUCLEON;
             k_morton<<<nb, VBLOCK, 0, st>>>(c->x, n, 1024.0 / c->p.xl[0], 1024.0 / c->p.xl[1],
-                                            1024.0 / c->p.xl[2], c->keys0, c->idx0);
+                                            1024.0 / c->p.xl[2], c->keys0, c->idx0, nuc ? c->zii : nullptr);
             size_t bytes = c->cub_bytes;
             cub::DeviceRadixSort::SortPairs(c->cub_tmp, bytes, c->keys0, c->keys1, c->idx0, c->perm, n,
-                                            0, 30, st);
+                                            0, nuc ? 31 : 30, st);
         }
         ++k;
         c->need_sort = false;
@@ -786,7 +785,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     // HBM admission: refuse up front rather than fail half-way.
     size_t cub_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned*)nullptr, (unsigned*)nullptr,
-                                    (int*)nullptr, (int*)nullptr, n, 0, 30);
+                                    (int*)nullptr, (int*)nullptr, n, 0, 31);
     size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
                    (sizeof(double4) + sizeof(float) * SHADOW_FLOATS / SHADOW_TILE) * ((size_t)n + SHADOW_TILE) + sizeof(int) * 5 * (size_t)n + cub_bytes +
                    sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;

@@ -64,15 +64,20 @@ __device__ __forceinline__ unsigned hilbert10(unsigned x0, unsigned x1, unsigned
 }
 
 // keys[i] = Hilbert index of particle i's cell on a 1024^3 grid over the box.
+// With species (nucleons: 1 = proton, 0 = neutron), bit 30 puts the protons
+// first: warps then hold one species, so the p-p Coulomb term, which reaches
+// every proton pair, runs on whole warps instead of the ~40 % of lanes that
+// are protons in a mixed warp.
 static __global__ void k_morton(const double* __restrict__ x, int n, double sx, double sy, double sz,
-                         unsigned* __restrict__ keys, int* __restrict__ idx)
+                         unsigned* __restrict__ keys, int* __restrict__ idx,
+                         const double* __restrict__ species = nullptr)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int cx = min(max((int)(x[3 * i] * sx), 0), 1023);
     const int cy = min(max((int)(x[3 * i + 1] * sy), 0), 1023);
     const int cz = min(max((int)(x[3 * i + 2] * sz), 0), 1023);
-    keys[i] = hilbert10(cx, cy, cz);
+    keys[i] = hilbert10(cx, cy, cz) | ((species && species[i] != 1.0) ? (1u << 30) : 0u);
     idx[i] = i;
 }
 
