@@ -166,6 +166,14 @@ YK_API int yk_get_state(yk_ctx* ctx, double* x, double* v, double* vold, double*
 YK_API int yk_set_state(yk_ctx* ctx, const double* x, const double* v,
                  const double* vold, const double* a);
 
+/* Potential energy per particle and pressure without touching the state:
+ * the energy-only routines vtot_ion_pure / vtot_ion_mix / vtot_nn
+ * (int_ion_pure.f:28-87, int_ion_mix.f:30-94, int_nn.f:37-119), which give
+ * the same ev and px as a measuring accel.  (The reference never calls them:
+ * its vtot dispatch has no caller.)  Runs one measuring force call into a
+ * side buffer, so the accelerations of the state stay as they are. */
+YK_API int yk_vtot(yk_ctx* ctx, double* ev, double* px);
+
 /* Asynchronous state snapshot for checkpoint and save_config
  * (md_utils.f:19-114, which write x and v, or x, v and a, through
  * rw_xvb.f:148-203).  yk_snapshot_begin copies the current x, v and a

@@ -131,3 +131,21 @@ def test_thermo_argument_checks(gpu):
         assert e.ttot() > 0.0
         with pytest.raises(Exception):
             e.strain((-1e6, NO, NO), list(p.xl))      # would make xl(1) negative
+
+
+@pytest.mark.parametrize("kind", ["pure", "mix", "nn"])
+def test_vtot_matches_oracle_and_keeps_state(gpu, orc, kind):
+    """yk_vtot against the oracle's restatement of vtot_* (energy per particle
+    and pressure, relative <= 1e-12), leaving the state's accelerations alone."""
+    w = {"pure": configs.pure_ion_ocp(87, 1500),
+         "mix": configs.ion_mixture_cfg(88, 2001),
+         "nn": configs.nucleon_matter(89, 1800)}[kind]
+    p = w.yk_params()
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        e.accel(False)
+        a0 = e.get_state()[3]
+        ev, px = e.vtot()
+        a1 = e.get_state()[3]
+    ev_ref, px_ref = orc.vtot(p, w.x, w.zii)
+    assert rel(ev, ev_ref) <= 1e-12 and rel(px, px_ref) <= 1e-12
+    assert np.array_equal(a0, a1)

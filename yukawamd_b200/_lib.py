@@ -34,6 +34,7 @@ SIGNATURES = {
     "yk_snapshot_begin": (C.c_int, [_ctx, _dp, _dp, _dp]),
     "yk_snapshot_wait": (C.c_int, [_ctx]),
     "yk_ttot": (C.c_int, [_ctx, _dp]),
+    "yk_vtot": (C.c_int, [_ctx, _dp, _dp]),
     "yk_tnorm": (C.c_int, [_ctx]),
     "yk_cancel_vcom": (C.c_int, [_ctx]),
     "yk_strain": (C.c_int, [_ctx, _dp, _dp, _dp]),

@@ -87,6 +87,7 @@ struct yk_ctx {
     // reductions and outputs
     double *fpart = nullptr, *kpart = nullptr;
     double *vpart = nullptr, *vsums = nullptr;   // ttot / tnorm / cancel_vcom sums
+    double* a_vtot = nullptr;                   // accelerations of yk_vtot (discarded)
     DevScalars* ds = nullptr;
     unsigned* err = nullptr;
     double* series = nullptr;
@@ -731,7 +732,7 @@ int yk_destroy(yk_ctx* c)
     void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->posf, c->perm, c->iperm,
                     c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->vpart, c->vsums,
                     c->ds, c->err,
-                    c->series, c->series_idx, c->job_counter, c->flush_buf, c->snap};
+                    c->series, c->series_idx, c->job_counter, c->flush_buf, c->snap, c->a_vtot};
     for (void* b : bufs) cudaFree(b);
     if (c->snap_taken) cudaEventDestroy(c->snap_taken);
     if (c->snap_done) cudaEventDestroy(c->snap_done);
@@ -930,6 +931,29 @@ int yk_accel(yk_ctx* c, int do_meas, double* a_out, yk_scalars* out)
     int rc = sync_and_check(c);
     if (rc) return rc;
     fill_scalars(c, out);
+    return YK_OK;
+}
+
+int yk_vtot(yk_ctx* c, double* ev, double* px)
+{
+    if (!c || !ev || !px) return fail(c, YK_ERR_ARG, "ctx, ev and px are required");
+    CK(c, cudaSetDevice(c->dev));
+    if (!c->a_vtot) CK(c, cudaMalloc(&c->a_vtot, sizeof(double) * 3 * (size_t)(c->n + 3)));
+    // a measuring force call whose accelerations go to a side buffer, so the
+    // state's a (which the next step's drift reads) is left as it was
+    int k = 0;
+    if (c->need_sort || c->pos_dirty) k += enqueue_order(c, c->need_sort);
+    std::swap(c->a, c->a_vtot);
+    k += enqueue_force(c, true);
+    k += enqueue_finish(c, true, 0, false);
+    std::swap(c->a, c->a_vtot);
+    g_launches += k;
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    yk_scalars s;
+    fill_scalars(c, &s);
+    *ev = s.ev;
+    *px = s.px;
     return YK_OK;
 }
 

@@ -135,6 +135,12 @@ class Engine:
         check(self._lib.yk_ttot(self._ctx, C.byref(out)), self._ctx)
         return out.value
 
+    def vtot(self):
+        """(ev, px) of the current positions; the accelerations are not changed."""
+        ev, px = C.c_double(), C.c_double()
+        check(self._lib.yk_vtot(self._ctx, C.byref(ev), C.byref(px)), self._ctx)
+        return ev.value, px.value
+
     def tnorm(self):
         check(self._lib.yk_tnorm(self._ctx), self._ctx)
 
