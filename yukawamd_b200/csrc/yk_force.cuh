@@ -304,13 +304,24 @@ __device__ __forceinline__ void phys32(const ForceArgs& fa, double wi, double wj
     }
 }
 
+// The reference's conditional minimum image on FP64 comparisons; the mixed
+// form uses it because its FP64 pipe is idle while its integer pipe is busy.
+__device__ __forceinline__ double min_image_cmp(double d, double L)
+{
+    const double hL = 0.5 * L;
+    double s = 0.0;
+    if (d > hL) s = -L;
+    else if (d < -hL) s = L;
+    return __dadd_rn(d, s);
+}
+
 template <int SIM, bool MEAS>
 __device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, const double4& pj,
                                        bool valid, PairOut<float>& o)
 {
-    o.dx = __double2float_rn(min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]));
-    o.dy = __double2float_rn(min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]));
-    o.dz = __double2float_rn(min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]));
+    o.dx = __double2float_rn(min_image_cmp(__dsub_rn(pi.x, pj.x), fa.xl[0]));
+    o.dy = __double2float_rn(min_image_cmp(__dsub_rn(pi.y, pj.y), fa.xl[1]));
+    o.dz = __double2float_rn(min_image_cmp(__dsub_rn(pi.z, pj.z), fa.xl[2]));
     phys32<SIM, MEAS>(fa, pi.w, pj.w, valid, o);
 }
 
