@@ -174,6 +174,16 @@ YK_API int yk_set_state(yk_ctx* ctx, const double* x, const double* v,
  * side buffer, so the accelerations of the state stay as they are. */
 YK_API int yk_vtot(yk_ctx* ctx, double* ev, double* px);
 
+/* The pair-distance histogram of the two-particle correlation function
+ * g(r): subroutine g with ig > 0 (g.f:55-66; its calls are commented out in
+ * md.F:64, 154, 184).  For every unique pair of the current positions,
+ * rr = pdist(i, j) (gen_utils.f:115-128) goes to bin
+ * min(nbin, int(fac2 rr + 1)), fac2 = 2 float(nbin) / sqrt(3) / min(xl), with
+ * the reference's arithmetic; the counts are ADDED to counts[0..nbin-1], as g
+ * accumulates gg(:, ig).  nbin <= 8192.  The normalization of g with
+ * ig = -1 (g.f:97-130) is host arithmetic: yukawamd_b200/gofr.py. */
+YK_API int yk_gofr_counts(yk_ctx* ctx, int nbin, double* counts);
+
 /* Asynchronous state snapshot for checkpoint and save_config
  * (md_utils.f:19-114, which write x and v, or x, v and a, through
  * rw_xvb.f:148-203).  yk_snapshot_begin copies the current x, v and a

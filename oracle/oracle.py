@@ -52,6 +52,7 @@ def _load(variant):
     lib.orc_thomas_fermi_xmuc.argtypes = [C.c_double, C.c_double, C.c_int]
     lib.orc_thomas_fermi_xmuc.restype = C.c_double
     lib.orc_vtot.argtypes = [P, C.c_int, _dp, _dp, _dp, _dp]
+    lib.orc_gofr_counts.argtypes = [P, C.c_int, _dp, C.c_int, _dp]
     lib.orc_set_threads.argtypes = [C.c_int]
     lib.orc_set_row_range.argtypes = [C.c_int, C.c_int]
     lib.orc_max_threads.restype = C.c_int
@@ -131,6 +132,14 @@ class Oracle:
 
     def thomas_fermi_xmuc(self, ztot, rho, n):
         return self.lib.orc_thomas_fermi_xmuc(ztot, rho, n)
+
+    def gofr_counts(self, params, x, nbin):
+        x = _f64(x)
+        counts = np.zeros(nbin)
+        rc = self.lib.orc_gofr_counts(C.byref(params), len(x) // 3, _ptr(x), int(nbin), _ptr(counts))
+        if rc:
+            raise RuntimeError("orc_gofr_counts failed")
+        return counts
 
     def vtot(self, params, x, zii=None):
         x = _f64(x)

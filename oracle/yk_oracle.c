@@ -833,3 +833,32 @@ int orc_vtot(const yk_params* p, int n, const double* x, const double* zii,
     *pressure = p->rho * (p->kT + (double)t1 / f_3n(n));
     return YK_OK;
 }
+
+/* The pair-distance histogram of subroutine g (g.f:55-66): for every unique
+ * pair, rr = pdist(i, j) (gen_utils.f:115-128: per axis min(|d|, xl - |d|),
+ * sqrt of the sum, plus the REAL*4 literal 1.e-15), bin ii = min(nbin,
+ * int(fac2*rr + 1)) with fac2 = 2.*float(nbin)/sqrt(3.)/xlmin evaluated as the
+ * Fortran does (REAL*4 up to the division by xlmin).  Adds 1 to counts[ii-1]. */
+int orc_gofr_counts(const yk_params* p, int n, const double* x, int nbin, double* counts)
+{
+    if (!p || !x || !counts || n < 1 || nbin < 1) return YK_ERR_ARG;
+    const double* xl = p->xl;
+    const double xlmin = fmin(xl[0], fmin(xl[1], xl[2]));
+    const float f4 = (2.0f * (float)nbin) / sqrtf(3.0f);
+    const double fac2 = (double)f4 / xlmin;
+    const double tiny = (double)1.e-15f;
+    for (int i = 0; i <= n - 2; ++i)
+        for (int j = i + 1; j <= n - 1; ++j) {
+            double rr = 0.;
+            for (int k = 0; k < 3; ++k) {
+                double yy = fabs(x[3 * i + k] - x[3 * j + k]);
+                yy = fmin(yy, xl[k] - yy);
+                rr = rr + yy * yy;
+            }
+            rr = sqrt(rr) + tiny;
+            int ii = (int)(fac2 * rr + 1.0);
+            if (ii > nbin) ii = nbin;
+            counts[ii - 1] += 1.0;
+        }
+    return YK_OK;
+}

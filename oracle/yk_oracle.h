@@ -55,6 +55,9 @@ void   orc_strain(const yk_params* p, int n, double* x, double* xl,
 double orc_rncut(double aa, double bb, double cc, double xpacket); /* :296-311 */
 double orc_thomas_fermi_xmuc(double ztot, double rho, int n);    /* :266-278 */
 
+/* g(r) pair-distance histogram of g.f:55-66, added to counts[0..nbin-1]. */
+int orc_gofr_counts(const yk_params* p, int n, const double* x, int nbin, double* counts);
+
 /* Energy-only routines (dead code in the reference; int_ion_pure.f:28-87,
  * int_ion_mix.f:30-94, int_nn.f:37-119).  Returns evavg and pressure. */
 int orc_vtot(const yk_params* p, int n, const double* x, const double* zii,

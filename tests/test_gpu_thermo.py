@@ -149,3 +149,24 @@ def test_vtot_matches_oracle_and_keeps_state(gpu, orc, kind):
     ev_ref, px_ref = orc.vtot(p, w.x, w.zii)
     assert rel(ev, ev_ref) <= 1e-12 and rel(px, px_ref) <= 1e-12
     assert np.array_equal(a0, a1)
+
+
+@pytest.mark.parametrize("kind,n", [("pure", 2000), ("mix", 1537), ("nn", 1300)])
+def test_gofr_counts_equal_oracle(gpu, orc, kind, n):
+    """yk_gofr_counts bins every pair as the reference's g does (g.f:55-66):
+    the counts equal the oracle's bin for bin, two calls add up, and the state
+    is untouched."""
+    w = {"pure": configs.pure_ion_ocp(91, n), "mix": configs.ion_mixture_cfg(92, n),
+         "nn": configs.nucleon_matter(93, n)}[kind]
+    p = w.yk_params()
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        e.run(3, 0, series=False)
+        x = e.get_state()[0]
+        for nbin in (50, 777, 8192):
+            c = e.gofr_counts(nbin)
+            assert np.array_equal(c, orc.gofr_counts(p, x, nbin)), nbin
+            e.gofr_counts(nbin, c)
+            assert np.array_equal(c, 2 * orc.gofr_counts(p, x, nbin))
+        assert np.array_equal(e.get_state()[0], x)
+        with pytest.raises(Exception):
+            e.gofr_counts(8193)

@@ -35,6 +35,7 @@ SIGNATURES = {
     "yk_snapshot_wait": (C.c_int, [_ctx]),
     "yk_ttot": (C.c_int, [_ctx, _dp]),
     "yk_vtot": (C.c_int, [_ctx, _dp, _dp]),
+    "yk_gofr_counts": (C.c_int, [_ctx, C.c_int, _dp]),
     "yk_tnorm": (C.c_int, [_ctx]),
     "yk_cancel_vcom": (C.c_int, [_ctx]),
     "yk_strain": (C.c_int, [_ctx, _dp, _dp, _dp]),

@@ -24,6 +24,7 @@
 #include "yk_force.cuh"
 #include "yk_internal.h"
 #include "yk_pairs.cuh"
+#include "yk_gofr.cuh"
 #include "yk_near.cuh"
 #include "yk_sort.cuh"
 #include "yk_thermo.cuh"
@@ -88,6 +89,8 @@ struct yk_ctx {
     double *fpart = nullptr, *kpart = nullptr;
     double *vpart = nullptr, *vsums = nullptr;   // ttot / tnorm / cancel_vcom sums
     double* a_vtot = nullptr;                   // accelerations of yk_vtot (discarded)
+    unsigned long long* gofr = nullptr;         // yk_gofr_counts histogram
+    int gofr_cap = 0;
     DevScalars* ds = nullptr;
     unsigned* err = nullptr;
     double* series = nullptr;
@@ -732,7 +735,7 @@ int yk_destroy(yk_ctx* c)
     void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->posf, c->perm, c->iperm,
                     c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->vpart, c->vsums,
                     c->ds, c->err,
-                    c->series, c->series_idx, c->job_counter, c->flush_buf, c->snap, c->a_vtot};
+                    c->series, c->series_idx, c->job_counter, c->flush_buf, c->snap, c->a_vtot, c->gofr};
     for (void* b : bufs) cudaFree(b);
     if (c->snap_taken) cudaEventDestroy(c->snap_taken);
     if (c->snap_done) cudaEventDestroy(c->snap_done);
@@ -954,6 +957,47 @@ int yk_vtot(yk_ctx* c, double* ev, double* px)
     fill_scalars(c, &s);
     *ev = s.ev;
     *px = s.px;
+    return YK_OK;
+}
+
+int yk_gofr_counts(yk_ctx* c, int nbin, double* counts)
+{
+    if (!c || !counts) return fail(c, YK_ERR_ARG, "ctx and counts are required");
+    if (nbin < 1 || nbin > GOFR_MAX_BINS) return fail(c, YK_ERR_ARG, "nbin must be 1..%d (got %d)", GOFR_MAX_BINS, nbin);
+    CK(c, cudaSetDevice(c->dev));
+    if (c->gofr_cap < nbin) {
+        if (c->gofr) CK(c, cudaFree(c->gofr));
+        c->gofr = nullptr;
+        c->gofr_cap = 0;
+        CK(c, cudaMalloc((void**)&c->gofr, sizeof(unsigned long long) * (size_t)nbin));
+        c->gofr_cap = nbin;
+    }
+    int k = 0;
+    if (c->need_sort || c->pos_dirty) k += enqueue_order(c, c->need_sort);
+    GofrArgs g{};
+    const double xlmin = std::min(c->p.xl[0], std::min(c->p.xl[1], c->p.xl[2]));
+    for (int d = 0; d < 3; ++d) g.xl[d] = c->p.xl[d];
+    const float f4 = (2.0f * (float)nbin) / std::sqrt(3.0f);     // REAL*4 in g.f:56
+    g.fac2 = (double)f4 / xlmin;
+    g.tiny = (double)1.e-15f;
+    g.nbin = nbin;
+    g.n = c->n;
+    g.M = (c->n + GOFR_BLOCK - 1) / GOFR_BLOCK;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+    const long long units = (long long)g.M * (g.M + 1) / 2;
+    const int grid = (int)std::min<long long>(units, 8LL * sms);
+    const size_t smem = GOFR_BLOCK * sizeof(double4) + sizeof(unsigned) * (size_t)nbin;
+    CK(c, cudaFuncSetAttribute(k_gofr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(c, cudaMemsetAsync(c->gofr, 0, sizeof(unsigned long long) * (size_t)nbin, c->stream));
+    k_gofr<<<grid, GOFR_BLOCK, smem, c->stream>>>(c->pos, g, c->gofr);
+    g_launches += k + 1;
+    std::vector<unsigned long long> h(nbin);
+    CK(c, cudaMemcpyAsync(h.data(), c->gofr, sizeof(unsigned long long) * (size_t)nbin, cudaMemcpyDeviceToHost,
+                          c->stream));
+    int rc = sync_and_check(c);
+    if (rc) return rc;
+    for (int b = 0; b < nbin; ++b) counts[b] += (double)h[b];
     return YK_OK;
 }
 

@@ -141,6 +141,15 @@ class Engine:
         check(self._lib.yk_vtot(self._ctx, C.byref(ev), C.byref(px)), self._ctx)
         return ev.value, px.value
 
+    def gofr_counts(self, nbin, counts=None):
+        """Add the pair-distance histogram of g(r) (g.f:55-66) of the current
+        positions to counts (float64[nbin], new zeros if None); returns it."""
+        counts = np.zeros(int(nbin)) if counts is None else counts
+        if counts.dtype != np.float64 or counts.size != int(nbin) or not counts.flags["C_CONTIGUOUS"]:
+            raise ValueError("counts must be a C-contiguous float64 array of nbin values")
+        check(self._lib.yk_gofr_counts(self._ctx, int(nbin), _ptr(counts)), self._ctx)
+        return counts
+
     def tnorm(self):
         check(self._lib.yk_tnorm(self._ctx), self._ctx)
 
