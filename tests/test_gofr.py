@@ -62,3 +62,19 @@ def test_ideal_gas_is_flat(tmp_path):
     write(tmp_path / "g.out", rr, gm, gs)
     line = open(tmp_path / "g.out").readline()
     assert len(line.rstrip("\n")) == 15 + 2 + 15 + 2 + 15
+
+
+def test_sofq_of_ideal_gas_is_one():
+    """S(q) of s.f on g = 1 everywhere is 1 for every q, and for a g with one
+    extra bump it follows the transform's formula term by term."""
+    g = GofR(nbin=40, ngroup=2)
+    g.gnorm = np.ones((40, 2))
+    q, sm, ss = g.sofq(1000, 0.05, [30.0, 30.0, 30.0], 0.2, 0.1, 12)
+    assert np.allclose(q, 0.2 + 0.1 * np.arange(12))
+    assert np.all(sm == 1.0) and np.all(ss == 0.0)
+    g.gnorm[5, :] = 2.0
+    q, sm, _ = g.sofq(1000, 0.05, [30.0, 30.0, 30.0], 0.2, 0.1, 3)
+    dd = 30.0 / 40 * float(np.float32(np.sqrt(3.0))) / 2
+    r5 = (6 - 0.5) * dd
+    want = 4 * np.pi * dd * 0.05 * r5 ** 2 * np.sin(q * r5) / (q * r5) + 1
+    assert np.allclose(sm, want, rtol=1e-12)

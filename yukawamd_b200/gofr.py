@@ -11,6 +11,9 @@ every particle as one species.  `GofR` restates its three phases:
             groups (g.f:97-130), with the reference's REAL*4 promotions
 
 and `write` prints the g.out lines (format 10000: f15.8, 2x, es15.8, 2x, es15.8).
+`GofR.sofq` is subroutine s (s.f:22-97), which md.F would call between g(-1)
+and g(-2): the static structure factor S(q) = 1 + rho 4 pi int r^2
+sin(qr)/(qr) (g(r) - 1) dr on the normalized g of every group.
 """
 import math
 
@@ -51,6 +54,7 @@ class GofR:
             rr[j - 1] = _f32(j - 0.5) * dd                    # (j-.5) is REAL*4
             for i in range(ngroup):
                 g[j - 1, i] = fac * self.gg[j - 1, i] / (self.cgg[i] + _f32(1.e-30)) / rr[j - 1] ** 2
+        self.gnorm = g                                       # gg(:,:,0) after g.f:106-111
         gmean = np.empty(nbin)
         gstd = np.empty(nbin)
         for j in range(nbin):
@@ -65,9 +69,46 @@ class GofR:
             gstd[j] = math.sqrt(abs(m2 - m ** 2) / ngroup)
         return rr, gmean, gstd
 
+    def sofq(self, n, rho, xl, qmin, dq, nsbin):
+        """s.f:22-97 on the groups normalized by finish().  Returns (q, smean, sstd)."""
+        nbin, ngroup = self.nbin, self.ngroup
+        nbmax = int(_f32(nbin / _f32(math.sqrt(3.0))))         # integer = REAL*4 quotient
+        xlmin = min(xl)
+        dd = xlmin / _f32(nbin) * _f32(math.sqrt(3.0)) / 2
+        ngspec = n
+        rhox = _f32(_f32(ngspec) / _f32(n)) * rho
+        r = [(_f32(k) - _f32(0.5)) * dd for k in range(1, nbmax + 1)]
+        ss = np.empty((nsbin, ngroup))
+        for i in range(ngroup):
+            q = qmin - dq
+            for j in range(nsbin):
+                q = q + dq
+                acc = 0.0
+                for k in range(nbmax):
+                    rq = q * r[k]
+                    acc = acc + (r[k] ** 2) * (math.sin(rq) / rq) * (self.gnorm[k, i] - 1.0)
+                ss[j, i] = 4.0 * PI * dd * rhox * acc + 1.0
+        qs = np.empty(nsbin)
+        smean = np.empty(nsbin)
+        sstd = np.empty(nsbin)
+        q = qmin - dq
+        for j in range(nsbin):
+            q = q + dq
+            m = 0.0
+            m2 = 0.0
+            for i in range(ngroup):
+                m += ss[j, i]
+                m2 += ss[j, i] ** 2
+            m = m / _f32(ngroup)
+            m2 = m2 / _f32(ngroup)
+            qs[j] = q
+            smean[j] = m
+            sstd[j] = math.sqrt(abs(m2 - m ** 2) / _f32(ngroup))
+        return qs, smean, sstd
+
 
 def write(path, rr, gmean, gstd):
-    """g.out lines of g.f:126 (format 10000)."""
+    """g.out lines of g.f:126 (format 10000); also the s.out lines of s.f:86."""
     with open(path, "w") as f:
         for a, b, c in zip(rr, gmean, gstd):
             f.write("%15.8f  %15.8E  %15.8E\n" % (a, b, c))
