@@ -98,3 +98,63 @@ def test_restated_exp_within_two_ulp():
 def test_underflow_flushes_to_zero():
     assert exp_neg_f32(100.0) == 0.0
     assert exp_neg_f32(1e5) == 0.0
+
+
+# ---- FP64 exp(-t) (exp_neg_f64, table-driven) ------------------------------
+
+def _f64_source_table():
+    text = open(SRC).read()
+    body = text[text.index("g_exp2_64[64] = {"):]
+    body = body[body.index("{") + 1:body.index("};")]
+    return [float(v) for v in body.replace("\n", " ").split(",") if v.strip()]
+
+
+def _fma64(a, b, c):
+    from fractions import Fraction
+    return float(Fraction(a) * Fraction(b) + Fraction(c))   # one rounding
+
+
+def exp_neg_f64(t):
+    import struct
+    tab = _f64_source_table()
+    MAG = 6755399441055744.0
+    kd = _fma64(-t, 92.33248261689366, MAG)
+    nf = kd - MAG
+    r = _fma64(-nf, 3.623510646634843e-19, _fma64(-nf, 0.010830424696249145, -t))
+    q = 1.0 / 120.0
+    for c in (1.0 / 24.0, 1.0 / 6.0, 0.5, 1.0):
+        q = _fma64(q, r, c)
+    p = q * r
+    bits = struct.unpack("<q", struct.pack("<d", kd))[0]
+    ni = ((bits & 0xffffffff) ^ 0x80000000) - 0x80000000      # low word as int32
+    tj = tab[ni & 63]
+    res = _fma64(tj, p, tj)
+    rb = struct.unpack("<q", struct.pack("<d", res))[0]
+    rb += (ni >> 6) << 52
+    return 0.0 if t > 700.0 else struct.unpack("<d", struct.pack("<q", rb))[0]
+
+
+def test_f64_table_is_correctly_rounded():
+    from decimal import Decimal, getcontext
+    getcontext().prec = 50
+    ln2 = Decimal(2).ln()
+    tab = _f64_source_table()
+    assert len(tab) == 64
+    for j, v in enumerate(tab):
+        assert v == float((Decimal(j) / 64 * ln2).exp())
+
+
+def test_f64_exp_within_three_ulp():
+    from decimal import Decimal, getcontext
+    getcontext().prec = 50
+    rng = np.random.default_rng(11)
+    ts = np.concatenate([[0.0, 1e-300, 1e-9, 0.5, 1.0, np.log(2.0) / 128, 10.0, 53.0, 699.0],
+                         rng.uniform(0.0, 12.0, 300), rng.uniform(0.0, 700.0, 100)])
+    worst = 0.0
+    for t in ts:
+        t = float(t)
+        got = exp_neg_f64(t)
+        ref = (-Decimal(t)).exp()
+        worst = max(worst, float(abs(Decimal(got) - ref) / Decimal(float(np.spacing(float(ref))))))
+    assert worst <= 3.0, worst
+    assert exp_neg_f64(701.0) == 0.0

@@ -196,6 +196,57 @@ __device__ __forceinline__ float exp_neg_f32(float t)
     return (k < -125.f) ? 0.f : r;
 }
 
+// ---- FP64 exp(-t), t >= 0 -----------------------------------------------
+// Table-driven method of P. T. P. Tang ("Table-driven implementation of the
+// exponential function in IEEE floating-point arithmetic", ACM TOMS 15,
+// 144-157, 1989): -t = (64 m + j) ln2/64 + r with |r| <= ln2/128, so
+// e^{-t} = 2^m 2^{j/64} e^r.  N = 64 m + j = rint(-t 64/ln2) comes from the
+// 1.5*2^52 add (its low word is N); r from two FMAs with ln2/64 split into a
+// double and its remainder; e^r - 1 from its Taylor polynomial to r^5
+// (truncation < 4e-17 relative); 2^{j/64} from a table of correctly rounded
+// doubles; 2^m through the exponent bits.  Error <= 3 ulp for t in [0, 700]
+// (tests/test_numerics.py restates it); results for t > 700 flush to zero.
+static __device__ const double g_exp2_64[64] = {
+    1.0, 1.0108892860517005, 1.0218971486541166, 1.0330248790212284,
+    1.0442737824274138, 1.0556451783605572, 1.0671404006768237, 1.0787607977571199,
+    1.0905077326652577, 1.102382583307841, 1.1143867425958924, 1.1265216186082418,
+    1.1387886347566916, 1.1511892299529827, 1.1637248587775775, 1.1763969916502812,
+    1.189207115002721, 1.202156731452703, 1.215247359980469, 1.22848053610687,
+    1.241857812073484, 1.255380757024691, 1.2690509571917332, 1.2828700160787783,
+    1.2968395546510096, 1.3109612115247644, 1.3252366431597413, 1.339667524053303,
+    1.3542555469368927, 1.3690024229745905, 1.383909881963832, 1.3989796725383112,
+    1.4142135623730951, 1.42961333839197, 1.4451808069770467, 1.460917794180647,
+    1.4768261459394993, 1.4929077282912648, 1.5091644275934228, 1.5255981507445384,
+    1.5422108254079407, 1.559004400237837, 1.5759808451078865, 1.593142151342267,
+    1.6104903319492543, 1.6280274218573478, 1.645755478153965, 1.6636765803267364,
+    1.681792830507429, 1.7001063537185235, 1.718619298122478, 1.7373338352737062,
+    1.7562521603732995, 1.7753764925265212, 1.7947090750031072, 1.8142521755003989,
+    1.8340080864093424, 1.8539791250833855, 1.8741676341103, 1.8945759815869656,
+    1.9152065613971474, 1.9360617934922943, 1.9571441241754002, 1.978456026387951,
+};
+
+__device__ __forceinline__ double exp_neg_f64(double t)
+{
+    const double MAG = 6755399441055744.0;                // 1.5 * 2^52
+    const double INV = 92.33248261689366;                 // 64 / ln 2
+    const double L1 = 0.010830424696249145;               // ln2/64, rounded
+    const double L2 = 3.623510646634843e-19;              // ln2/64 - L1
+    const double kd = __fma_rn(-t, INV, MAG);
+    const double nf = __dsub_rn(kd, MAG);
+    const double r = __fma_rn(-nf, L2, __fma_rn(-nf, L1, -t));
+    double q = 1.0 / 120.0;
+    q = __fma_rn(q, r, 1.0 / 24.0);
+    q = __fma_rn(q, r, 1.0 / 6.0);
+    q = __fma_rn(q, r, 0.5);
+    q = __fma_rn(q, r, 1.0);
+    const double p = __dmul_rn(q, r);                     // e^r - 1
+    const int ni = __double2loint(kd);
+    const double tj = __ldg(&g_exp2_64[ni & 63]);
+    const double res = __fma_rn(tj, p, tj);
+    const int hi = __double2hiint(res) + ((ni >> 6) << 20);
+    return t > 700.0 ? 0.0 : __hiloint2double(hi, __double2loint(res));
+}
+
 // FP32 1/sqrt(x): hardware estimate plus one Newton step.
 __device__ __forceinline__ float rsqrt_f32(float x)
 {

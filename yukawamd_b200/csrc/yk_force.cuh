@@ -15,8 +15,9 @@
 //         u = (aa e + B) e, fs = (2 aa e + B) e / Lambda, B = bb +/- cc by
 //         species equality; Coulomb (p-p, r^2 <= rccut^2): vc x the ion terms.
 //
-// PREC_FP64: all FP64 (exp(), rsqrt() from the CUDA math library; rsqrt
-// replaces the reference's sqrt and divide, 1/(r r^2) = rinv^3).
+// PREC_FP64: all FP64 (exp_neg_f64, our table-driven exp, and rsqrt() from
+// the CUDA math library; rsqrt replaces the reference's sqrt and divide,
+// 1/(r r^2) = rinv^3).
 // PREC_MIXED: displacement and minimum image in FP64, then cast to FP32; the
 // r^2, rsqrt, exp and force terms in FP32.
 //
@@ -205,7 +206,7 @@ __device__ __forceinline__ void phys64(const ForceArgs& fa, double wi, double wj
             const double rinv = rsqrt(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;
-            const double er = exp(-mr) * rinv;                // e^{-mu r}/r
+            const double er = exp_neg_f64(mr) * rinv;                // e^{-mu r}/r
             o.fs = (1.0 + mr) * er * (rinv * rinv);           // (1+mu r) e^{-mu r}/r^3
             if constexpr (MEAS) {
                 o.u = er - fa.evcut;
@@ -216,7 +217,7 @@ __device__ __forceinline__ void phys64(const ForceArgs& fa, double wi, double wj
     } else {
         if (!valid) return;
         if (fa.nuclear_on && r2 <= fa.rn2) {
-            const double e = exp(-(r2 * fa.xp2i));
+            const double e = exp_neg_f64(r2 * fa.xp2i);
             const double B = (wi == wj) ? fa.bpc : fa.bmc;
             const double fn = fa.xpi * (fa.aa2 * e + B) * e;
             o.fs = fn;
@@ -230,7 +231,7 @@ __device__ __forceinline__ void phys64(const ForceArgs& fa, double wi, double wj
             const double rinv = rsqrt(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;
-            const double er = fa.vc * exp(-mr) * rinv;         // vc e^{-mu r}/r
+            const double er = fa.vc * exp_neg_f64(mr) * rinv;         // vc e^{-mu r}/r
             const double fc = (1.0 + mr) * er * (rinv * rinv);
             o.fs += fc;
             if constexpr (MEAS) {
@@ -358,7 +359,7 @@ __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& 
         const double rinv = rsqrt(r2s);
         const double r = r2s * rinv;
         const double mr = fa.xmuc * r;
-        const double er = exp(-mr) * rinv;
+        const double er = exp_neg_f64(mr) * rinv;
         const double fs = (1.0 + mr) * er * (rinv * rinv);
         o.fs = hit ? fs : 0.0;
         o.u = (MEAS && hit) ? er - fa.evcut : 0.0;
