@@ -257,3 +257,35 @@ def test_nonfinite_state_rejected(gpu):
         with pytest.raises(Exception) as ei:
             e.set_state(x=bad)
         assert ei.value.code == abi.YK_ERR_NONFINITE
+
+
+def _reshaped(w, stretch, rccut=None):
+    """The workload in a rectangular box (edges scaled by `stretch`, positions
+    with them) and optionally another cutoff."""
+    import copy
+    w2 = copy.deepcopy(w)
+    x = w2.x.reshape(-1, 3) * np.asarray(stretch)
+    w2.x = np.ascontiguousarray(x.reshape(-1))
+    w2.params["xl"] = [w.params["xl"][k] * stretch[k] for k in range(3)]
+    if rccut is not None:
+        w2.params["rccut"] = rccut
+    return w2
+
+
+@pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
+@pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["rectangular", "cutoff-at-half-box", "no-cutoff"])
+def test_box_shapes_and_cutoffs(gpu, orc, case, prec, kern):
+    """Rectangular boxes (edges 2 : 1 : 0.7) and cutoffs at or beyond L/2, where
+    pairs straddle the minimum-image boundary: the per-pair screen's image
+    integers are then not used (the exact comparisons run), and the bounding-box
+    and near-list classifications meet ambiguous sources."""
+    w = configs.ion_mixture_cfg(101, 2500)
+    L = w.params["xl"][0]
+    if case == "rectangular":
+        w = _reshaped(w, (2.0, 1.0, 0.7))
+    elif case == "cutoff-at-half-box":
+        w = _reshaped(w, (1.0, 1.0, 1.0), rccut=0.5 * L)
+    else:
+        w = _reshaped(w, (1.3, 1.0, 0.8), rccut=1e50)
+    check_accel(orc, w, prec, True, mix_mode=abi.YK_MIX_FIXED, tuning=KERNELS[kern])
