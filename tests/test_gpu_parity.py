@@ -289,3 +289,26 @@ def test_box_shapes_and_cutoffs(gpu, orc, case, prec, kern):
     else:
         w = _reshaped(w, (1.3, 1.0, 0.8), rccut=1e50)
     check_accel(orc, w, prec, True, mix_mode=abi.YK_MIX_FIXED, tuning=KERNELS[kern])
+
+
+@pytest.mark.parametrize("integ,bfield", [(1, 0.0), (3, 0.0), (2, 2.0e17), (3, 2.0e17)],
+                         ids=["vv1", "vv3", "vv2-b", "vv3-b"])
+def test_run_graph_equals_newton_loop_integrators(gpu, integ, bfield):
+    """yk_run's CUDA graphs for the other integrators and the B field give the
+    same bits as the same steps through yk_newton."""
+    w = configs.ion_mixture_cfg(52, 1200)
+    p = w.yk_params(integrator=integ, bfield=bfield)
+    steps, me = 60, 7
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e1:
+        e1.accel(True)
+        ser1 = [abi.YkScalars.from_buffer_copy(e1.newton(g % me == 0)) for g in range(1, steps + 1)]
+        st1 = e1.get_state()
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e2:
+        e2.set_tuning(graph_steps=20)
+        e2.accel(True)
+        ser2 = e2.run(steps, me)
+        st2 = e2.get_state()
+    for A, B in zip(st1, st2):
+        assert np.array_equal(A, B)
+    for s1, s2 in zip(ser1, ser2):
+        assert bytes(s1) == bytes(s2)
