@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -467,6 +468,38 @@ extern "C" {
 
 const char* yk_batch_last_error(const yk_batch* b) { return b ? b->errmsg.c_str() : g_batch_err.c_str(); }
 
+// Batches are created and destroyed often (the serving loop rebuilds a group
+// whenever its membership changes), so their device arrays come from the
+// device's stream-ordered memory pool, which keeps up to POOL_KEEP bytes of
+// freed memory cached between batches: a rebuild then costs no cudaMalloc /
+// cudaFree round trips to the driver.
+constexpr uint64_t POOL_KEEP = 8ull << 30;
+
+static void pool_setup(int dev)
+{
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = POOL_KEEP;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done.push_back(dev);
+}
+
+// Bytes the pool holds cached but unused (free for the next batch).
+static size_t pool_cached(int dev)
+{
+    cudaMemPool_t pool;
+    uint64_t reserved = 0, used = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    return reserved > used ? (size_t)(reserved - used) : 0;
+}
+
 // Job table and target-side scratch layout for segment length seg: a job is
 // (box, target block R, segment s) over at most seg source tiles; jobs run
 // costliest first.  Fills the descriptors' seg, nseg, Si_off, sm_off, njobs.
@@ -529,14 +562,14 @@ int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t)
     std::vector<int4> sorted;
     long long si = 0;
     layout_jobs(b, seg, sorted, si);
-    cudaFree(b->Si);
-    cudaFree(b->Sm);
-    cudaFree(b->jobs);
+    cudaFreeAsync(b->Si, b->stream);
+    cudaFreeAsync(b->Sm, b->stream);
+    cudaFreeAsync(b->jobs, b->stream);
     b->Si = b->Sm = nullptr;
     b->jobs = nullptr;
-    if (cudaMalloc((void**)&b->Si, sizeof(double) * (size_t)std::max<long long>(si, 1)) != cudaSuccess ||
-        cudaMalloc((void**)&b->Sm, sizeof(double) * 8 * (size_t)std::max(b->njobs, 1)) != cudaSuccess ||
-        cudaMalloc((void**)&b->jobs, sizeof(int4) * (size_t)std::max(b->njobs, 1)) != cudaSuccess)
+    if (cudaMallocAsync((void**)&b->Si, sizeof(double) * (size_t)std::max<long long>(si, 1), b->stream) != cudaSuccess ||
+        cudaMallocAsync((void**)&b->Sm, sizeof(double) * 8 * (size_t)std::max(b->njobs, 1), b->stream) != cudaSuccess ||
+        cudaMallocAsync((void**)&b->jobs, sizeof(int4) * (size_t)std::max(b->njobs, 1), b->stream) != cudaSuccess)
         return bfail(b, YK_ERR_NOMEM, "re-allocating the job scratch for pair_seg %d failed", seg);
     BCK(b, cudaMemcpyAsync(b->rd, b->hrd.data(), sizeof(RepDesc) * b->nrep, cudaMemcpyHostToDevice, b->stream));
     BCK(b, cudaMemcpyAsync(b->jobs, sorted.data(), sizeof(int4) * sorted.size(), cudaMemcpyHostToDevice,
@@ -554,7 +587,11 @@ int yk_batch_destroy(yk_batch* b)
                     b->posf,  b->perm,  b->iperm, b->keys0,  b->keys1,   b->idx0,    b->idx1,   b->cub_tmp,
                     b->rd,    b->jobs,  b->counter, b->tile_rep, b->vblocks, b->Si, b->Sj,   b->Sm,
                     b->kpart, b->ds,    b->err,   b->series, b->series_idx};
-    for (void* p : bufs) cudaFree(p);
+    if (b->stream) {
+        for (void* p : bufs)
+            if (p) cudaFreeAsync(p, b->stream);            // back to the pool
+        cudaStreamSynchronize(b->stream);
+    }
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -677,17 +714,24 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
                         sizeof(unsigned long long) * 2 * ntot + cub_bytes + sizeof(RepDesc) * nrep +
                         sizeof(int4) * b->njobs + (64u << 20);
     size_t free_b = 0, total_b = 0;
+    pool_setup(device);
     cudaMemGetInfo(&free_b, &total_b);
+    free_b += pool_cached(device);
     if (need > free_b) {
         delete b;
         return bfail(nullptr, YK_ERR_NOMEM, "batch needs %zu bytes, %zu free", need, free_b);
     }
 
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        yk_batch_destroy(b);
+        return bfail(nullptr, YK_ERR_CUDA, "stream creation failed");
+    }
 #define BALLOC(ptr, cnt)                                                                    \
     do {                                                                                    \
-        if (cudaMalloc((void**)&(ptr), sizeof(*(ptr)) * (size_t)std::max<long long>((cnt), 1)) != cudaSuccess) { \
+        if (cudaMallocAsync((void**)&(ptr), sizeof(*(ptr)) * (size_t)std::max<long long>((cnt), 1), b->stream) != \
+            cudaSuccess) {                                                                  \
             yk_batch_destroy(b);                                                            \
-            return bfail(nullptr, YK_ERR_NOMEM, "cudaMalloc of " #ptr " failed");           \
+            return bfail(nullptr, YK_ERR_NOMEM, "device allocation of " #ptr " failed");    \
         }                                                                                   \
     } while (0)
     BALLOC(b->x, 3 * ntot);
@@ -719,8 +763,7 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
     BALLOC(b->series_idx, 1);
 #undef BALLOC
     b->cub_bytes = cub_bytes;
-    if (cudaMalloc(&b->cub_tmp, std::max<size_t>(cub_bytes, 16)) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaMallocAsync(&b->cub_tmp, std::max<size_t>(cub_bytes, 16), b->stream) != cudaSuccess ||
         cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) {
         yk_batch_destroy(b);
         return bfail(nullptr, YK_ERR_NOMEM, "batch set-up failed");
@@ -803,10 +846,10 @@ int yk_batch_run(yk_batch* b, int nsteps, int meas_every, yk_scalars* series, do
     const bool want = series != nullptr;
     if (want && b->series_cap < nsteps) {
         drop_graphs_b(b);
-        cudaFree(b->series);
+        cudaFreeAsync(b->series, b->stream);
         b->series = nullptr;
         b->series_cap = 0;
-        BCK(b, cudaMalloc((void**)&b->series, sizeof(double) * 13 * (size_t)nsteps * b->nrep));
+        BCK(b, cudaMallocAsync((void**)&b->series, sizeof(double) * 13 * (size_t)nsteps * b->nrep, b->stream));
         b->series_cap = nsteps;
     }
     cudaStream_t st = b->stream;

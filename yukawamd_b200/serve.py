@@ -105,6 +105,8 @@ class Server:
         self.budget = hbm_budget
         self.groups = {}          # (kind, precision) -> (Batch, [Request])
         self.finished = []
+        self.rebuilds = 0         # group rebuilds and the wall time spent in them
+        self.rebuild_s = 0.0
 
     # -- group management ----------------------------------------------
     def _rebuild(self, key, runs):
@@ -212,12 +214,15 @@ class Server:
 
     def _sync_groups(self, active):
         """Rebuild exactly the groups whose membership changed."""
+        t = time.perf_counter()
         keys = set((r.kind, r.precision) for r in active) | set(self.groups)
         for key in keys:
             want = [r for r in active if (r.kind, r.precision) == key]
             have = self.groups[key][1] if key in self.groups else []
             if [r.rid for r in want] != [r.rid for r in have]:
                 self._rebuild(key, want)
+                self.rebuilds += 1
+        self.rebuild_s += time.perf_counter() - t
 
     def report(self, wall, pairs_done):
         lat = np.array([r.latency for r in self.finished if r.shadow_of < 0])
@@ -225,7 +230,8 @@ class Server:
                "pairs_per_s": pairs_done / wall if wall > 0 else 0.0,
                "latency_p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
                "latency_p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
-               "latency_max_s": float(lat.max()) if len(lat) else None}
+               "latency_max_s": float(lat.max()) if len(lat) else None,
+               "group_rebuilds": self.rebuilds, "rebuild_wall_s": self.rebuild_s}
         shadows = []
         by_id = {r.rid: r for r in self.finished}
         for r in self.finished:
