@@ -196,6 +196,33 @@ __device__ __forceinline__ float exp_neg_f32(float t)
     return (k < -125.f) ? 0.f : r;
 }
 
+// ---- FP32 exp(-t), t >= 0, on the hardware base-2 exponential ----------
+// e^{-t} = 2^{yh} 2^{yl} with yh = fl(-t log2 e) and yl the rest of the
+// exact product (the FMA-recovered rounding error of yh plus -t times the
+// low part of log2 e); 2^{yl} = 1 + yl ln 2 to first order (|yl| < 2^-24
+// |yh|, so the dropped term is below 1e-13 for t < 90).  2^{yh} is the
+// ex2.approx.ftz.f32 instruction of the transcendental unit.  Used where that
+// unit has spare issue slots; the result is within the instruction's error
+// (about 2 ulp) of e^{-t}; results below 2^-126 flush to zero.
+__device__ __forceinline__ float ex2_approx(float y)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+    return r;
+}
+
+__device__ __forceinline__ float exp_neg_f32_xu(float t)
+{
+    const float L2E_HI = 1.44269502162933349609375f;      // float(log2 e)
+    const float L2E_LO_LN2 = 1.3349758e-8f;              // (log2 e - L2E_HI) ln 2
+    const float LN2 = 0.693147180559945309f;
+    const float yh = -t * L2E_HI;
+    const float e1 = fmaf(-t, L2E_HI, -yh);              // exact error of -t*L2E_HI
+    const float c = fmaf(e1, LN2, -t * L2E_LO_LN2);      // yl ln 2
+    const float r = ex2_approx(yh);
+    return fmaf(r, c, r);
+}
+
 // ---- FP64 exp(-t), t >= 0 -----------------------------------------------
 // Table-driven method of P. T. P. Tang ("Table-driven implementation of the
 // exponential function in IEEE floating-point arithmetic", ACM TOMS 15,

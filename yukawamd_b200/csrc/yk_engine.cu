@@ -210,11 +210,13 @@ static void setup_args(yk_ctx* c)
     f.bpcf = (float)f.bpc;
     f.bmcf = (float)f.bmc;
     // FP32 screen: widen each radius by 2^-19 L (16 ulp of the FP32 box
-    // coordinates; the shadow displacement is off by at most ~5 ulp) and the
-    // squares by a relative 2^-20 (three FP32 roundings of r^2 are 2e-7).
+    // coordinates; the FP32 arithmetic of the shadow displacement is off by at
+    // most ~5 ulp) plus 4 SHADOW_Q (the hi parts are on the SHADOW_Q grid, so
+    // a displacement taken from them is off by up to SHADOW_Q per axis), and
+    // the squares by a relative 2^-20 (three FP32 roundings of r^2 are 2e-7).
     {
         const double Lmax = std::max(p.xl[0], std::max(p.xl[1], p.xl[2]));
-        const double delta = Lmax * std::ldexp(1.0, -19);
+        const double delta = Lmax * std::ldexp(1.0, -19) + 4.0 * SHADOW_Q;
         const double grow = 1.0 + std::ldexp(1.0, -20);
         auto widen2 = [&](double r) {
             const double rs = (r + delta) * grow;
@@ -224,6 +226,9 @@ static void setup_args(yk_ctx* c)
         for (int k = 0; k < 3; ++k) {
             f.Lf[k] = (float)p.xl[k];
             f.invLf[k] = (float)(1.0 / p.xl[k]);
+            const double h = shadow_hi(p.xl[k]);
+            f.Lh[k] = (float)h;
+            f.Ll[k] = (float)(p.xl[k] - h);
         }
         f.scr_c2 = (p.sim_type == YK_SIM_NUCLEON && !p.coulomb_on) ? -1.0f : widen2(p.rccut);
         f.scr_n2 = (p.sim_type == YK_SIM_NUCLEON && p.nuclear_on) ? widen2(p.rncut) : -1.0f;
@@ -234,7 +239,11 @@ static void setup_args(yk_ctx* c)
         // them instead of the exact comparisons.
         const double Lmin = std::min(p.xl[0], std::min(p.xl[1], p.xl[2]));
         const double rscr = std::sqrt(std::max((double)f.scr_c2, (double)f.scr_n2));
-        f.img_k = (std::isfinite(rscr) && rscr + std::ldexp(Lmax, -14) < 0.5 * Lmin) ? 1 : 0;
+        f.img_k = (std::isfinite(rscr) && rscr + std::ldexp(Lmax, -14) + 4.0 * SHADOW_Q < 0.5 * Lmin) ? 1 : 0;
+        // The hi/lo displacement is exact up to its last rounding while every
+        // coordinate and box length is below SHADOW_EXACT; a margin of 2 leaves
+        // room for coordinates up to 2 L.
+        f.lo = (f.img_k && 2.0 * Lmax < SHADOW_EXACT) ? 1 : 0;
     }
     f.n = c->n;
     f.nuclear_on = p.nuclear_on;

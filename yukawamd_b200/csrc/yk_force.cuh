@@ -18,8 +18,12 @@
 // PREC_FP64: all FP64 (exp_neg_f64, our table-driven exp, and rsqrt() from
 // the CUDA math library; rsqrt replaces the reference's sqrt and divide,
 // 1/(r r^2) = rinv^3).
-// PREC_MIXED: displacement and minimum image in FP64, then cast to FP32; the
-// r^2, rsqrt, exp and force terms in FP32.
+// PREC_MIXED: the r^2, rsqrt, exp and force terms in FP32.  Ion pairs take
+// their displacement from the shadow's hi/lo parts (screen_d_x2: exact FP32
+// hi-part differences plus a lo correction, no FP64 arithmetic) and e^{-mu r}
+// from the hardware base-2 exponential (exp_neg_f32_xu) when the box allows
+// it (fa.lo); otherwise, and for nucleons, the displacement and minimum
+// image are FP64, then cast to FP32.
 //
 // Particles are addressed by "slot": the engine keeps them in a Morton
 // (space-filling-curve) order so that the 32 targets of a warp are close in
@@ -60,40 +64,75 @@ struct ForceArgs {
     float scr_c2, scr_n2;
     int n, nuclear_on, coulomb_on, mix_compat;
     int img_k;                       // the screen's image integers are exact (see setup)
+    // mixed form, ions: the displacement from the hi/lo shadow parts
+    // (screen_d_x2); Lh = box on the SHADOW_Q grid, Ll = box - Lh
+    float Lh[3], Ll[3];
+    int lo;                          // img_k and every box length below SHADOW_EXACT / 2
 };
 
 // FP32 shadow positions ("posf") are stored tile by tile: tile t (slots
-// 128t .. 128t+127) is a contiguous block of SHADOW_FLOATS = 896 floats, one
-// 256-float section per coordinate and then w[128].  Within a coordinate's
-// section each group of 4 slots s0..s3 takes 8 floats in the order
+// 128t .. 128t+127) is a contiguous block of SHADOW_FLOATS = 1664 floats:
+//   [0, 768)      hi parts of x, y, z, one 256-float section per coordinate
+//   [768, 896)    w[128] (charge / species word)
+//   [896, 1664)   lo parts of x, y, z, one 256-float section per coordinate
+// Within a coordinate's section each group of 4 slots s0..s3 takes 8 floats
+// in the order
 //     s0 s1 s1 s0 s2 s3 s3 s2
 // so that (a) two neighbouring slots (j, j+1), j even, are one aligned
 // float2 at offset 2j, and (b) every ordered pair of a group's halves that
 // the half-pair kernel's lane swizzle needs -- (s0,s1) (s1,s0) (s2,s3)
 // (s3,s2) -- is one aligned float2 at offset 2q, q = 0..3, in the block.
-// A source tile is one 3.5 KB bulk copy.
+//
+// hi = x rounded to the grid of SHADOW_Q = 2^-9 fm, lo = x - hi (|lo| <=
+// 2^-10, rounded to FP32).  On that grid every coordinate, box length and
+// difference below SHADOW_EXACT = 2^24 SHADOW_Q = 32768 fm is an FP32 number,
+// so the hi-part displacement x_j - x_i and its image shift by the grid box
+// length are exact FP32 operations; the mixed form adds the lo parts to get
+// the displacement to FP32 precision without any FP64 arithmetic
+// (screen_d_x2).  The screen and the FP64 form read only the first 896 floats
+// (one 3.5 KB bulk copy per tile); the mixed form also copies the lo part.
 constexpr int SHADOW_TILE = 128;
-constexpr int SHADOW_FLOATS = 7 * SHADOW_TILE;
+constexpr int SHADOW_HI_FLOATS = 7 * SHADOW_TILE;
+constexpr int SHADOW_LO_FLOATS = 6 * SHADOW_TILE;
+constexpr int SHADOW_FLOATS = SHADOW_HI_FLOATS + SHADOW_LO_FLOATS;
+constexpr double SHADOW_Q = 1.0 / 512.0;
+constexpr double SHADOW_EXACT = 32768.0;
 __host__ __device__ __forceinline__ int shadow_off(int j, int comp)
 {
-    return comp < 3 ? comp * 2 * SHADOW_TILE + 8 * (j >> 2) + ((j & 1) | ((j & 2) << 1))
-                    : 6 * SHADOW_TILE + j;
+    // comp 0..2: hi x, y, z; 3: w; 4..6: lo x, y, z
+    const int paired = 8 * (j >> 2) + ((j & 1) | ((j & 2) << 1));
+    return comp < 3 ? comp * 2 * SHADOW_TILE + paired
+                    : comp == 3 ? 6 * SHADOW_TILE + j : SHADOW_HI_FLOATS + (comp - 4) * 2 * SHADOW_TILE + paired;
 }
-// index of slot's (first) copy of component comp; the second copy of
-// comp < 3 is at shadow_index ^ 3
+// index of slot's (first) copy of component comp; the second copy of a
+// coordinate part (comp != 3) is at shadow_index ^ 3
 __host__ __device__ __forceinline__ long long shadow_index(int slot, int comp)
 {
     return (long long)(slot >> 7) * SHADOW_FLOATS + shadow_off(slot & (SHADOW_TILE - 1), comp);
 }
 
-__device__ __forceinline__ void store_shadow(float* __restrict__ posf, int slot, float x, float y, float z, float w)
+// hi part of a coordinate: the nearest multiple of SHADOW_Q (exact FP64
+// arithmetic: scaling by a power of two and rint)
+__host__ __device__ __forceinline__ double shadow_hi(double x)
 {
-    const float v[3] = {x, y, z};
+    return rint(x * (1.0 / SHADOW_Q)) * SHADOW_Q;
+}
+
+__device__ __forceinline__ void store_shadow(float* __restrict__ posf, int slot, double x, double y, double z,
+                                             float w)
+{
+    const double v[3] = {x, y, z};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+        const double h = shadow_hi(v[c]);
+        const float hf = __double2float_rn(h);
+        const float lf = __double2float_rn(__dsub_rn(v[c], h));
         const long long k = shadow_index(slot, c);
-        posf[k] = v[c];
-        posf[k ^ 3] = v[c];
+        posf[k] = hf;
+        posf[k ^ 3] = hf;
+        const long long kl = shadow_index(slot, 4 + c);
+        posf[kl] = lf;
+        posf[kl ^ 3] = lf;
     }
     posf[shadow_index(slot, 3)] = w;
 }
@@ -164,6 +203,37 @@ __device__ __forceinline__ float2 screen_r2k_x2(const ForceArgs& fa, const Scree
         float2 dc = __fadd2_rn(xj, make_float2(ni[c], ni[c]));
         k[c] = __fadd2_rn(__ffma2_rn(dc, make_float2(fa.invLf[c], fa.invLf[c]), MAG), NMAG);
         d[c] = __ffma2_rn(make_float2(-fa.Lf[c], -fa.Lf[c]), k[c], dc);
+    }
+    float2 r2 = __fmul2_rn(d[2], d[2]);
+    r2 = __ffma2_rn(d[1], d[1], r2);
+    return __ffma2_rn(d[0], d[0], r2);
+}
+
+// The mixed form's displacement for the ordered source pair at offset off
+// of group g (the order of screen_r2k_x2): d = x_j - x_i in the minimum
+// image, to FP32 precision, without FP64 arithmetic.  The hi-part difference
+// dc and its image shift dc - k Lh are exact (every value is a multiple of
+// SHADOW_Q below SHADOW_EXACT); the lo parts and the box's lo part go into
+// one correction term, and the sum is the one rounding.  t is the hi tile, tl
+// the lo tile (x, y, z sections of 256 paired floats); nli holds the target's
+// negated lo parts.  Returns r^2.
+__device__ __forceinline__ float2 screen_d_x2(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
+                                              const float* __restrict__ t, const float* __restrict__ tl, int g,
+                                              int off, float2 (&d)[3])
+{
+    const float2 MAG = make_float2(12582912.0f, 12582912.0f);
+    const float2 NMAG = make_float2(-12582912.0f, -12582912.0f);
+    const float ni[3] = {si.nx, si.ny, si.nz};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float2 xj = *reinterpret_cast<const float2*>(t + c * 2 * SHADOW_TILE + 8 * g + off);
+        const float2 lj = *reinterpret_cast<const float2*>(tl + c * 2 * SHADOW_TILE + 8 * g + off);
+        const float2 dc = __fadd2_rn(xj, make_float2(ni[c], ni[c]));
+        const float2 k = __fadd2_rn(__ffma2_rn(dc, make_float2(fa.invLf[c], fa.invLf[c]), MAG), NMAG);
+        const float2 d1 = __ffma2_rn(make_float2(-fa.Lh[c], -fa.Lh[c]), k, dc);
+        float2 e = __fadd2_rn(lj, make_float2(nli[c], nli[c]));
+        e = __ffma2_rn(make_float2(-fa.Ll[c], -fa.Ll[c]), k, e);
+        d[c] = __fadd2_rn(d1, e);
     }
     float2 r2 = __fmul2_rn(d[2], d[2]);
     r2 = __ffma2_rn(d[1], d[1], r2);
@@ -384,6 +454,28 @@ __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& 
     }
 }
 
+// The mixed form's ion pair from screen_d_x2's displacement dj = x_j - x_i
+// and r^2 (hit: the pair is selected and inside r_c), branch-free as
+// ion_pair_nb.
+template <bool MEAS>
+__device__ __forceinline__ void ion_pair_f32(const ForceArgs& fa, float r2, bool hit, float djx, float djy,
+                                             float djz, PairOut<float>& o)
+{
+    o.dx = -djx;
+    o.dy = -djy;
+    o.dz = -djz;
+    const float r2s = hit ? r2 : 1.0f;
+    const float rinv = rsqrt_f32(r2s);
+    const float r = r2s * rinv;
+    const float mr = fa.xmucf * r;
+    const float er = exp_neg_f32_xu(mr) * rinv;
+    const float fs = (1.0f + mr) * er * (rinv * rinv);
+    o.fs = hit ? fs : 0.f;
+    o.u = (MEAS && hit) ? er - fa.evcutf : 0.f;
+    o.w = (MEAS && hit) ? fs * r2 : 0.f;
+    o.hit = hit;
+}
+
 // ---- per-target accumulators --------------------------------------------
 // FP64 form: plain double sums.  Mixed form: Knuth two-sum FP32 sums.
 template <int PREC, bool MEAS>
@@ -543,7 +635,7 @@ __device__ __forceinline__ void store_accel(const ForceArgs& fa, int orig, doubl
 
 // Shared memory of k_force_rows: 2 stages of FTILE double4 and one shadow tile,
 // 2 mbarriers and the block-reduction scratch.
-constexpr int FORCE_SMEM = 2 * FTILE * (int)sizeof(double4) + 2 * SHADOW_FLOATS * (int)sizeof(float) + 16 +
+constexpr int FORCE_SMEM = 2 * FTILE * (int)sizeof(double4) + 2 * SHADOW_HI_FLOATS * (int)sizeof(float) + 16 +
                            32 * NSCAL * (int)sizeof(double);
 
 template <int SIM, int PREC, bool MEAS>
@@ -555,8 +647,8 @@ k_force_rows(const double4* __restrict__ pos, const float* __restrict__ posf,
     extern __shared__ __align__(128) unsigned char smem[];
     double4* tile = reinterpret_cast<double4*>(smem);
     float* tilef = reinterpret_cast<float*>(smem + 2 * FTILE * sizeof(double4));
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * FTILE * sizeof(double4) + 2 * SHADOW_FLOATS * sizeof(float));
-    double* red = reinterpret_cast<double*>(smem + 2 * FTILE * sizeof(double4) + 2 * SHADOW_FLOATS * sizeof(float) + 16);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * FTILE * sizeof(double4) + 2 * SHADOW_HI_FLOATS * sizeof(float));
+    double* red = reinterpret_cast<double*>(smem + 2 * FTILE * sizeof(double4) + 2 * SHADOW_HI_FLOATS * sizeof(float) + 16);
 
     const int n = fa.n;
     const int i = blockIdx.x * FBLOCK + threadIdx.x;
@@ -575,11 +667,11 @@ k_force_rows(const double4* __restrict__ pos, const float* __restrict__ posf,
         const int j0 = t * FTILE;
         const int cnt = min(FTILE, n - j0);
         const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
-        const unsigned bytesf = (unsigned)SHADOW_FLOATS * (unsigned)sizeof(float);
+        const unsigned bytesf = (unsigned)SHADOW_HI_FLOATS * (unsigned)sizeof(float);
         uint64_t* b = &bar[t & 1];
         mbar_arrive_expect_tx(b, bytes + bytesf);
         bulk_g2s(tile + (t & 1) * FTILE, pos + j0, bytes, b);
-        bulk_g2s(tilef + (t & 1) * SHADOW_FLOATS, posf + (size_t)t * SHADOW_FLOATS, bytesf, b);
+        bulk_g2s(tilef + (t & 1) * SHADOW_HI_FLOATS, posf + (size_t)t * SHADOW_FLOATS, bytesf, b);
     };
     if (threadIdx.x == 0) {
         issue(0);
@@ -603,7 +695,7 @@ k_force_rows(const double4* __restrict__ pos, const float* __restrict__ posf,
         const int j0 = t * FTILE;
         const int cnt = min(FTILE, n - j0);
         const double4* tl = tile + st * FTILE;
-        const float* tlf = tilef + st * SHADOW_FLOATS;
+        const float* tlf = tilef + st * SHADOW_HI_FLOATS;
         if (active) {
 #pragma unroll 2
             for (int jj = 0; jj < cnt; ++jj) {

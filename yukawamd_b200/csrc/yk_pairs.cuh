@@ -174,6 +174,67 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
     }
 }
 
+// pair_group for ions in the mixed form when the box allows the FP32
+// displacement (fa.lo): the screen computes the final displacement and r^2
+// (screen_d_x2), so its mask is the cutoff test itself and the pair terms
+// need no FP64 source tile.  tll is the tile's lo part, nli the target's
+// negated lo parts.
+template <int SIM, bool MEAS, bool CHECK>
+__device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
+                                              float wi, const float* tlf, const float* tll, int j0, int jlim,
+                                              bool diag, bool active, int tid, int sw,
+                                              TargetAcc<PREC_MIXED, MEAS>& acc, double* my_acc)
+{
+    const int g = j0 >> 2;
+    float2 da[3], db[3];
+    const float2 ra = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * sw, da);
+    const float2 rb = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * (sw ^ 2), db);
+    unsigned m = (ra.x <= fa.rc2f ? 1u : 0u) | (ra.y <= fa.rc2f ? 2u : 0u) | (rb.x <= fa.rc2f ? 4u : 0u) |
+                 (rb.y <= fa.rc2f ? 8u : 0u);
+    if constexpr (CHECK) {
+        unsigned ok = 0;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const int jl = j0 + (jj ^ sw);
+            if (active && jl < jlim && (!diag || jl > tid)) ok |= 1u << jj;
+        }
+        m &= ok;
+    }
+    if (!__any_sync(0xffffffffu, m != 0)) return;
+    const float* tw = tlf + 6 * SHADOW_TILE + j0;
+    float r[4][3];
+    GroupSum<PREC_MIXED, MEAS> gs;
+    gs.zero();
+    bool any = false;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+        const float2* dp = jj < 2 ? da : db;
+        const bool second = (jj & 1) != 0;
+        const float r2 = jj == 0 ? ra.x : jj == 1 ? ra.y : jj == 2 ? rb.x : rb.y;
+        PairOut<float> o;
+        ion_pair_f32<MEAS>(fa, r2, ((m >> jj) & 1u) != 0, second ? dp[0].y : dp[0].x,
+                           second ? dp[1].y : dp[1].x, second ? dp[2].y : dp[2].x, o);
+        gs.add(o, SIM == SIM_MIX ? tw[jj ^ sw] : 1.0f);
+        const float fsj = o.fs * wi;                 // 0 unless the pair interacts
+        r[jj][0] = fsj * o.dx;
+        r[jj][1] = fsj * o.dy;
+        r[jj][2] = fsj * o.dz;
+        any |= o.hit;
+    }
+    acc.add_group(gs);
+    if (__any_sync(0xffffffffu, any)) {
+        float t[3];
+        reduce_scatter4(r, t);
+        const int lane = threadIdx.x & 31;
+        const int jl = j0 + sw;
+        if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
+            my_acc[3 * jl] -= (double)t[0];
+            my_acc[3 * jl + 1] -= (double)t[1];
+            my_acc[3 * jl + 2] -= (double)t[2];
+        }
+    }
+}
+
 // ---- which source groups can reach a warp's targets ----------------------
 // The bounding box of a warp's active targets (FP32 copies), computed once per
 // job; a source farther than the screening radius from the box (in the
@@ -225,7 +286,9 @@ __device__ __forceinline__ bool box_reaches(const ForceArgs& fa, const WarpBox& 
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float L = fa.Lf[k];
-        const float mu = 3.814697265625e-6f * L;                 // 2^-18 L
+        // 2^-18 L for the FP32 arithmetic, plus 2 SHADOW_Q for the grid
+        // rounding of the shadow coordinate
+        const float mu = fmaf(3.814697265625e-6f, L, (float)(2.0 * SHADOW_Q));
         const float lo = (b.lo[k] - x[k]) - mu;                  // x_i - x_j over the box
         const float hi = (b.hi[k] - x[k]) + mu;
         // distance from 0 to [lo, hi] + s L, the smallest over s = -1, 0, 1
@@ -278,8 +341,8 @@ __device__ __forceinline__ unsigned near_groups(const ForceArgs& fa, const WarpB
 
 // Shared memory of the half-pair kernels.
 struct PairSmem {
-    double4 tile[2][PB];                  // FP64 source tiles (TMA)
-    float tilef[2][SHADOW_FLOATS];        // FP32 shadow source tiles (TMA)
+    double4 tile[2][PB];                  // FP64 source tiles, or the shadow lo parts (TMA)
+    float tilef[2][SHADOW_HI_FLOATS];     // FP32 shadow source tiles, hi parts and w (TMA)
     double acc_j[2][PWARPS][PB * 3];      // per-warp reaction rows, one set per tile stage
     double red[32 * NSCAL];               // block reduction scratch
     uint64_t bar[2];                      // one mbarrier per tile stage
@@ -305,7 +368,7 @@ __device__ __forceinline__ void pairs_smem_init(PairSmem& sm)
     // filled.  Zero them once: from then on every slot holds a finite position
     // (zero, or one left by an earlier tile) and a masked pair yields 0, not NaN.
     for (int k = threadIdx.x; k < 2 * PB; k += blockDim.x) (&sm.tile[0][0])[k] = make_double4(0.0, 0.0, 0.0, 0.0);
-    for (int k = threadIdx.x; k < 2 * SHADOW_FLOATS; k += blockDim.x) (&sm.tilef[0][0])[k] = 0.f;
+    for (int k = threadIdx.x; k < 2 * SHADOW_HI_FLOATS; k += blockDim.x) (&sm.tilef[0][0])[k] = 0.f;
     if (threadIdx.x == 0) {
         mbar_init(&sm.bar[0], 1);
         mbar_init(&sm.bar[1], 1);
@@ -316,17 +379,23 @@ __device__ __forceinline__ void pairs_smem_init(PairSmem& sm)
     __syncthreads();
 }
 
-// Load source tile C of box bx into stage qq & 1 (one thread).
-__device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int C, unsigned qq)
+static_assert(SHADOW_LO_FLOATS * sizeof(float) <= PB * sizeof(double4), "lo parts must fit a tile stage");
+
+// Load source tile C of box bx into stage qq & 1 (one thread): the shadow hi
+// parts, and the FP64 positions or (lo) the shadow lo parts.
+__device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int C, unsigned qq, bool lo)
 {
     const int j0 = C * PB;
     const int cnt = min(PB, bx.n - j0);
-    const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
-    const unsigned bytesf = (unsigned)SHADOW_FLOATS * (unsigned)sizeof(float);
+    const unsigned bytes = lo ? (unsigned)SHADOW_LO_FLOATS * (unsigned)sizeof(float)
+                              : (unsigned)cnt * (unsigned)sizeof(double4);
+    const unsigned bytesf = (unsigned)SHADOW_HI_FLOATS * (unsigned)sizeof(float);
+    const float* src = bx.posf + (size_t)C * SHADOW_FLOATS;
     uint64_t* b = &sm.bar[qq & 1];
     mbar_arrive_expect_tx(b, bytes + bytesf);
-    bulk_g2s(&sm.tile[qq & 1][0], bx.pos + j0, bytes, b);
-    bulk_g2s(&sm.tilef[qq & 1][0], bx.posf + (size_t)C * SHADOW_FLOATS, bytesf, b);
+    if (lo) bulk_g2s(&sm.tile[qq & 1][0], src + SHADOW_HI_FLOATS, bytes, b);
+    else bulk_g2s(&sm.tile[qq & 1][0], bx.pos + j0, bytes, b);
+    bulk_g2s(&sm.tilef[qq & 1][0], src, bytesf, b);
 }
 
 // Job (R, sg) of box bx: target block R against source tiles
@@ -364,12 +433,20 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
     const WarpBox box = warp_box(pi, active);
     TargetAcc<PREC, MEAS> acc;
     acc.zero();
+    // mixed-form ions on a box that allows it: FP32 displacements from the
+    // shadow's hi/lo parts, no FP64 source tiles
+    const bool lo = (PREC == PREC_MIXED) && (SIM == SIM_PURE || SIM == SIM_MIX) && fa.lo != 0;
+    float nli[3] = {0.f, 0.f, 0.f};
+    if (lo) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nli[c] = -bx.posf[shadow_index(active ? i : 0, 4 + c)];
+    }
 
     // both stages are free: every warp has passed the block barrier that
     // handed out this job
     if (tid == 0) {
-        pairs_issue(sm, bx, C0, q);
-        if (C0 + 1 < C1) pairs_issue(sm, bx, C0 + 1, q + 1);
+        pairs_issue(sm, bx, C0, q, lo);
+        if (C0 + 1 < C1) pairs_issue(sm, bx, C0 + 1, q + 1, lo);
     }
     const unsigned q0 = q;
     for (int C = C0; C < C1; ++C, ++q) {
@@ -385,7 +462,20 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
         __syncwarp();
         // on the diagonal tile only sources after the warp's first target count
         unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, diag ? 32 * warp + 1 : 0);
-        if (!diag && jlim == PB && all_active) {
+        if (lo) {
+            if constexpr (PREC == PREC_MIXED && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+                const float* tll = reinterpret_cast<const float*>(tl);
+                if (!diag && jlim == PB && all_active) {
+                    for (; gm; gm &= gm - 1)
+                        pair_group_lo<SIM, MEAS, false>(fa, si, nli, wi, tlf, tll, 4 * (__ffs(gm) - 1), jlim,
+                                                        diag, active, tid, sw, acc, my_acc);
+                } else {
+                    for (; gm; gm &= gm - 1)
+                        pair_group_lo<SIM, MEAS, true>(fa, si, nli, wi, tlf, tll, 4 * (__ffs(gm) - 1), jlim,
+                                                       diag, active, tid, sw, acc, my_acc);
+                }
+            }
+        } else if (!diag && jlim == PB && all_active) {
             for (; gm; gm &= gm - 1)
                 pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
                                                    active, tid, sw, acc, my_acc);
@@ -412,7 +502,7 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
                 dj[k] = v;
             }
             __syncwarp();
-            if (lane == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2);
+            if (lane == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2, lo);
         }
     }
     q = q0 + (unsigned)(C1 - C0);

@@ -93,7 +93,7 @@ static __global__ void k_apply_perm(const int* __restrict__ perm, int* __restric
     iperm[o] = s;
     const double4 p = make_double4(x[3 * o], x[3 * o + 1], x[3 * o + 2], pack_w ? zii[o] : 0.0);
     pos[s] = p;
-    store_shadow(posf, s, (float)p.x, (float)p.y, (float)p.z, (float)p.w);
+    store_shadow(posf, s, p.x, p.y, p.z, (float)p.w);
 }
 
 }  // namespace yk

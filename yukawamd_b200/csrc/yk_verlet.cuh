@@ -45,7 +45,7 @@ __device__ __forceinline__ void store_pos(double4* pos, float* posf, int slot, c
                                           double w)
 {
     pos[slot] = make_double4(xn[0], xn[1], xn[2], w);
-    store_shadow(posf, slot, (float)xn[0], (float)xn[1], (float)xn[2], (float)w);
+    store_shadow(posf, slot, xn[0], xn[1], xn[2], (float)w);
 }
 
 // x = x + v dt + afac a, wrapped once (vel_verlet_2.f:36-42)
