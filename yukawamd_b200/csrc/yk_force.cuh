@@ -465,7 +465,7 @@ __device__ __forceinline__ void ion_pair_f32(const ForceArgs& fa, float r2, bool
     o.dy = -djy;
     o.dz = -djz;
     const float r2s = hit ? r2 : 1.0f;
-    const float rinv = rsqrt_f32(r2s);
+    const float rinv = rsqrtf(r2s);                    // hardware estimate, no Newton step
     const float r = r2s * rinv;
     const float mr = fa.xmucf * r;
     const float er = exp_neg_f32_xu(mr) * rinv;

@@ -62,6 +62,31 @@ __device__ __forceinline__ double to_f64(real_t<PREC> v)
     return (double)v;
 }
 
+// FP32 form of reduce_scatter4 below with the adds paired into FP32x2
+// instructions (the same sums in the same order).
+__device__ __forceinline__ void reduce_scatter4(float (&r)[4][3], float (&t)[3])
+{
+    float2 a[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        a[c] = __fadd2_rn(make_float2(r[0][c], r[1][c]),
+                          make_float2(__shfl_xor_sync(0xffffffffu, r[2][c], 16),
+                                      __shfl_xor_sync(0xffffffffu, r[3][c], 16)));
+    float2 t01 = __fadd2_rn(make_float2(a[0].x, a[1].x),
+                            make_float2(__shfl_xor_sync(0xffffffffu, a[0].y, 8),
+                                        __shfl_xor_sync(0xffffffffu, a[1].y, 8)));
+    float t2 = a[2].x + __shfl_xor_sync(0xffffffffu, a[2].y, 8);
+#pragma unroll
+    for (int m = 4; m > 0; m >>= 1) {
+        t01 = __fadd2_rn(t01, make_float2(__shfl_xor_sync(0xffffffffu, t01.x, m),
+                                          __shfl_xor_sync(0xffffffffu, t01.y, m)));
+        t2 += __shfl_xor_sync(0xffffffffu, t2, m);
+    }
+    t[0] = t01.x;
+    t[1] = t01.y;
+    t[2] = t2;
+}
+
 // Reduce-scatter of four 3-vectors held in lane-swizzled slots (slot q of
 // lane L belongs to source q ^ sw(L)).  On return t[] holds the warp-wide sum
 // for source sw(L).  T is double for the FP64 form and float for the mixed
@@ -167,9 +192,11 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
         const int lane = threadIdx.x & 31;
         const int jl = j0 + sw;
         if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
-            my_acc[3 * jl] -= (double)t[0];
-            my_acc[3 * jl + 1] -= (double)t[1];
-            my_acc[3 * jl + 2] -= (double)t[2];
+            // a warp visits each group of a tile once, so this is the row
+            // entry's only write (rows start at zero for skipped groups)
+            my_acc[3 * jl] = -(double)t[0];
+            my_acc[3 * jl + 1] = -(double)t[1];
+            my_acc[3 * jl + 2] = -(double)t[2];
         }
     }
 }
@@ -228,9 +255,11 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
         const int lane = threadIdx.x & 31;
         const int jl = j0 + sw;
         if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
-            my_acc[3 * jl] -= (double)t[0];
-            my_acc[3 * jl + 1] -= (double)t[1];
-            my_acc[3 * jl + 2] -= (double)t[2];
+            // a warp visits each group of a tile once, so this is the row
+            // entry's only write (rows start at zero for skipped groups)
+            my_acc[3 * jl] = -(double)t[0];
+            my_acc[3 * jl + 1] = -(double)t[1];
+            my_acc[3 * jl + 2] = -(double)t[2];
         }
     }
 }
