@@ -476,6 +476,25 @@ __device__ __forceinline__ void ion_pair_f32(const ForceArgs& fa, float r2, bool
     o.hit = hit;
 }
 
+// ion_pair_f32's terms for two pairs at once (the FP32 arithmetic paired):
+// r2 their r^2, msk 1 for a pair that interacts and 0 otherwise.  Returns fs
+// (0 for a masked pair) and, when measuring, u and w.
+template <bool MEAS>
+__device__ __forceinline__ void ion_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2& fs, float2& u,
+                                             float2& w)
+{
+    const float2 r2s = make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f);
+    const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
+    const float2 mr = __fmul2_rn(make_float2(fa.xmucf, fa.xmucf), __fmul2_rn(r2s, rinv));
+    const float2 er = __fmul2_rn(exp_neg_f32_xu_x2(mr), rinv);
+    const float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(make_float2(1.0f, 1.0f), mr), er), __fmul2_rn(rinv, rinv));
+    fs = __fmul2_rn(f, msk);
+    if constexpr (MEAS) {
+        u = __fmul2_rn(__fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf)), msk);
+        w = __fmul2_rn(fs, r2);
+    }
+}
+
 // ---- per-target accumulators --------------------------------------------
 // FP64 form: plain double sums.  Mixed form: Knuth two-sum FP32 sums.
 template <int PREC, bool MEAS>
@@ -588,6 +607,16 @@ struct TargetAcc<PREC_MIXED, MEAS> {
         if constexpr (MEAS) {
 #pragma unroll
             for (int k = 0; k < NSCAL; ++k) s[k].add(g.s[k]);
+        }
+    }
+    // add_group with the compensated sums advanced two at a time
+    __device__ __forceinline__ void add_group2(const GroupSum<PREC_MIXED, MEAS>& g)
+    {
+        cf32_add2(f[0], f[1], make_float2(g.f[0], g.f[1]));
+        f[2].add(g.f[2]);
+        if constexpr (MEAS) {
+#pragma unroll
+            for (int k = 0; k < NSCAL; k += 2) cf32_add2(s[k], s[k + 1], make_float2(g.s[k], g.s[k + 1]));
         }
     }
     __device__ __forceinline__ double force(int k) const { return f[k].value(); }

@@ -63,15 +63,15 @@ __device__ __forceinline__ double to_f64(real_t<PREC> v)
 }
 
 // FP32 form of reduce_scatter4 below with the adds paired into FP32x2
-// instructions (the same sums in the same order).
-__device__ __forceinline__ void reduce_scatter4(float (&r)[4][3], float (&t)[3])
+// instructions (the same sums in the same order); ra holds slots 0 and 1,
+// rb slots 2 and 3.
+__device__ __forceinline__ void reduce_scatter4_x2(const float2 (&ra)[3], const float2 (&rb)[3], float (&t)[3])
 {
     float2 a[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-        a[c] = __fadd2_rn(make_float2(r[0][c], r[1][c]),
-                          make_float2(__shfl_xor_sync(0xffffffffu, r[2][c], 16),
-                                      __shfl_xor_sync(0xffffffffu, r[3][c], 16)));
+        a[c] = __fadd2_rn(ra[c], make_float2(__shfl_xor_sync(0xffffffffu, rb[c].x, 16),
+                                             __shfl_xor_sync(0xffffffffu, rb[c].y, 16)));
     float2 t01 = __fadd2_rn(make_float2(a[0].x, a[1].x),
                             make_float2(__shfl_xor_sync(0xffffffffu, a[0].y, 8),
                                         __shfl_xor_sync(0xffffffffu, a[1].y, 8)));
@@ -85,6 +85,17 @@ __device__ __forceinline__ void reduce_scatter4(float (&r)[4][3], float (&t)[3])
     t[0] = t01.x;
     t[1] = t01.y;
     t[2] = t2;
+}
+
+__device__ __forceinline__ void reduce_scatter4(float (&r)[4][3], float (&t)[3])
+{
+    float2 ra[3], rb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        ra[c] = make_float2(r[0][c], r[1][c]);
+        rb[c] = make_float2(r[2][c], r[3][c]);
+    }
+    reduce_scatter4_x2(ra, rb, t);
 }
 
 // Reduce-scatter of four 3-vectors held in lane-swizzled slots (slot q of
@@ -228,39 +239,60 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
         m &= ok;
     }
     if (!__any_sync(0xffffffffu, m != 0)) return;
+    // The four pairs in two FP32x2 halves: a = steps 0, 1 and b = steps 2, 3
+    // (the screen's ra, da and rb, db).  d = x_j - x_i, so the target's terms
+    // carry a minus sign: F_i += fs Z_j (x_i - x_j) = -fs Z_j d
+    // (int_ion_mix.f:179), and the reaction on j is fs Z_i d (:180).
     const float* tw = tlf + 6 * SHADOW_TILE + j0;
-    float r[4][3];
+    const float2 mska = make_float2((m & 1u) ? 1.f : 0.f, (m & 2u) ? 1.f : 0.f);
+    const float2 mskb = make_float2((m & 4u) ? 1.f : 0.f, (m & 8u) ? 1.f : 0.f);
+    float2 fsa, ua, wa, fsb, ub, wb;
+    ion_terms_x2<MEAS>(fa, ra, mska, fsa, ua, wa);
+    ion_terms_x2<MEAS>(fa, rb, mskb, fsb, ub, wb);
+    const float2 wja = (SIM == SIM_MIX) ? make_float2(tw[sw], tw[sw ^ 1]) : make_float2(1.f, 1.f);
+    const float2 wjb = (SIM == SIM_MIX) ? make_float2(tw[sw ^ 2], tw[sw ^ 3]) : make_float2(1.f, 1.f);
+    const float2 ga = __fmul2_rn(fsa, wja), gb = __fmul2_rn(fsb, wjb);
     GroupSum<PREC_MIXED, MEAS> gs;
-    gs.zero();
-    bool any = false;
+    float2 fxa[3], fxb[3];
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-        const float2* dp = jj < 2 ? da : db;
-        const bool second = (jj & 1) != 0;
-        const float r2 = jj == 0 ? ra.x : jj == 1 ? ra.y : jj == 2 ? rb.x : rb.y;
-        PairOut<float> o;
-        ion_pair_f32<MEAS>(fa, r2, ((m >> jj) & 1u) != 0, second ? dp[0].y : dp[0].x,
-                           second ? dp[1].y : dp[1].x, second ? dp[2].y : dp[2].x, o);
-        gs.add(o, SIM == SIM_MIX ? tw[jj ^ sw] : 1.0f);
-        const float fsj = o.fs * wi;                 // 0 unless the pair interacts
-        r[jj][0] = fsj * o.dx;
-        r[jj][1] = fsj * o.dy;
-        r[jj][2] = fsj * o.dz;
-        any |= o.hit;
+    for (int c = 0; c < 3; ++c) {
+        fxa[c] = __fmul2_rn(ga, da[c]);
+        fxb[c] = __fmul2_rn(gb, db[c]);
+        const float2 sc = __fadd2_rn(fxa[c], fxb[c]);
+        gs.f[c] = -(sc.x + sc.y);
     }
-    acc.add_group(gs);
-    if (__any_sync(0xffffffffu, any)) {
-        float t[3];
-        reduce_scatter4(r, t);
-        const int lane = threadIdx.x & 31;
-        const int jl = j0 + sw;
-        if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
-            // a warp visits each group of a tile once, so this is the row
-            // entry's only write (rows start at zero for skipped groups)
-            my_acc[3 * jl] = -(double)t[0];
-            my_acc[3 * jl + 1] = -(double)t[1];
-            my_acc[3 * jl + 2] = -(double)t[2];
+    if constexpr (MEAS) {
+        const float2 su = __ffma2_rn(ub, wjb, __fmul2_rn(ua, wja));
+        const float2 sv = __ffma2_rn(wb, wjb, __fmul2_rn(wa, wja));
+        gs.s[0] = su.x + su.y;
+        gs.s[1] = sv.x + sv.y;
+        // pressure tensor d (x) (fs Z_j d): the two minus signs cancel
+        const int P[6] = {0, 0, 0, 1, 1, 2}, Q[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float2 sp = __ffma2_rn(db[P[k]], fxb[Q[k]], __fmul2_rn(da[P[k]], fxa[Q[k]]));
+            gs.s[2 + k] = sp.x + sp.y;
         }
+    }
+    acc.add_group2(gs);
+    const float2 wi2 = make_float2(wi, wi);
+    const float2 ha = __fmul2_rn(fsa, wi2), hb = __fmul2_rn(fsb, wi2);
+    float2 ra3[3], rb3[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        ra3[c] = __fmul2_rn(ha, da[c]);
+        rb3[c] = __fmul2_rn(hb, db[c]);
+    }
+    float t[3];
+    reduce_scatter4_x2(ra3, rb3, t);
+    const int lane = threadIdx.x & 31;
+    const int jl = j0 + sw;
+    if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
+        // a warp visits each group of a tile once, so this is the row
+        // entry's only write (rows start at zero for skipped groups)
+        my_acc[3 * jl] = (double)t[0];
+        my_acc[3 * jl + 1] = (double)t[1];
+        my_acc[3 * jl + 2] = (double)t[2];
     }
 }
 
