@@ -162,14 +162,14 @@ k_b_post(const int2* __restrict__ vb, const RepDesc* __restrict__ rd, double* __
     if constexpr (KIN) block_sum_store<NKIN>(tk, red, kpart + (size_t)blockIdx.x * NKIN);
 }
 
-template <int SIM, int PREC, bool MEAS>
-__global__ void __launch_bounds__(PB, 5)
+template <int SIM, int PREC, bool MEAS, bool LO = false>
+__global__ void __launch_bounds__(PB, (pairs_ctas_per_sm<PREC, LO>()))
 k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ posf,
                     const int4* __restrict__ jobs, int njobs, int* __restrict__ counter,
                     const RepDesc* __restrict__ rd, double* __restrict__ Si, double* __restrict__ Sj,
                     double* __restrict__ Sm, unsigned* __restrict__ err)
 {
-    __shared__ __align__(128) PairSmem sm;
+    __shared__ __align__(128) PairSmem<row_t<PREC>> sm;
     __shared__ __align__(16) ForceArgs sfa;
     __shared__ int4 sjob;
     pairs_smem_init(sm);
@@ -195,8 +195,8 @@ k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ p
         bx.M = d->T;
         bx.seg = d->seg;
         bx.nseg_max = d->nseg;
-        if (!pairs_job<SIM, PREC, MEAS>(sm, sfa, bx, jb.y, jb.z, Sm + (size_t)(d->sm_off + jb.w) * NSCAL,
-                                        err, q))
+        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 2>(sm, sfa, bx, jb.y, jb.z,
+                                                    Sm + (size_t)(d->sm_off + jb.w) * NSCAL, err, q))
             return;
     }
 }
@@ -295,7 +295,8 @@ struct yk_batch {
     double* series = nullptr;
     int series_cap = 0;
     int* series_idx = nullptr;
-    int force_grid = 0;
+    int force_grid = 0, force_grid_lo = 0;
+    bool all_lo = false;            // every box allows the mixed ion hi/lo displacement (fa.lo)
     int seg = BATCH_SEG, graph_steps = BATCH_GRAPH_STEPS;
     std::vector<RepDesc> hrd;       // host copy of the descriptors
     bool need_sort = true, pos_dirty = false;
@@ -346,14 +347,27 @@ template <int SIM, int PREC, bool MEAS>
 static int launch_force_b(yk_batch* b)
 {
     if (b->force_grid == 0) {
-        int per_sm = 0, sms = 0;
+        int per_sm = 0, per_sm_lo = 0, sms = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs_batch<SIM, PREC, MEAS>, PB, 0);
+        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lo, k_force_pairs_batch<SIM, PREC, MEAS, true>,
+                                                          PB, 0);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
         b->force_grid = std::max(1, per_sm) * std::max(1, sms);
+        b->force_grid_lo = std::max(1, per_sm_lo) * std::max(1, sms);
     }
     cudaMemsetAsync(b->counter, 0, sizeof(int), b->stream);
-    k_force_pairs_batch<SIM, PREC, MEAS><<<std::min(b->force_grid, b->njobs), PB, 0, b->stream>>>(
-        b->pos, b->posf, b->jobs, b->njobs, b->counter, b->rd, b->Si, b->Sj, b->Sm, b->err);
+    bool launched = false;
+    if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON) {
+        if (b->all_lo) {
+            k_force_pairs_batch<SIM, PREC, MEAS, true><<<std::min(b->force_grid_lo, b->njobs), PB, 0, b->stream>>>(
+                b->pos, b->posf, b->jobs, b->njobs, b->counter, b->rd, b->Si, b->Sj, b->Sm, b->err);
+            launched = true;
+        }
+    }
+    if (!launched)
+        k_force_pairs_batch<SIM, PREC, MEAS><<<std::min(b->force_grid, b->njobs), PB, 0, b->stream>>>(
+            b->pos, b->posf, b->jobs, b->njobs, b->counter, b->rd, b->Si, b->Sj, b->Sm, b->err);
     k_b_combine<SIM><<<(b->stot + 255) / 256, 256, 0, b->stream>>>(b->tile_rep, b->rd, b->Si, b->Sj, b->perm,
                                                                    b->zii, b->aii, b->a, b->stot);
     return 2;
@@ -699,6 +713,8 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
     std::vector<int4> sorted;
     layout_jobs(b, BATCH_SEG, sorted, si);
     b->nvb = (int)vblocks.size();
+    b->all_lo = !nuc;
+    for (int r = 0; r < nrep; ++r) b->all_lo = b->all_lo && rd[r].fa.lo != 0;
     int bits = 1;
     while ((1 << bits) < nrep) ++bits;
     b->key_bits = (nuc ? 31 : 30) + bits;
@@ -710,7 +726,7 @@ int yk_batch_create(int nrep, const yk_params* params, const int* n, const doubl
                                     b->key_bits);
     const size_t need = sizeof(double) * (size_t)(9 * ntot + A + 2 * ntot + sj + si + 8LL * b->njobs +
                                                   (long long)NKIN * b->nvb) +
-                        sizeof(double4) * stot + sizeof(float) * 7 * stot + sizeof(int) * (3 * ntot + 2 * stot) +
+                        sizeof(double4) * stot + sizeof(float) * (SHADOW_FLOATS / SHADOW_TILE) * stot + sizeof(int) * (3 * ntot + 2 * stot) +
                         sizeof(unsigned long long) * 2 * ntot + cub_bytes + sizeof(RepDesc) * nrep +
                         sizeof(int4) * b->njobs + (64u << 20);
     size_t free_b = 0, total_b = 0;

@@ -433,6 +433,14 @@ static int enqueue_order(yk_ctx* c, bool sort)
     return k + 1;
 }
 
+// The mixed ion kernels have a variant that always takes the hi/lo shadow
+// displacement (k_force_pairs<..., true>), for boxes that allow it.
+template <int SIM, int PREC>
+static bool lo_path(const ForceArgs& fa)
+{
+    return PREC == PREC_MIXED && SIM != SIM_NUCLEON && fa.lo != 0;
+}
+
 template <int SIM, int PREC, bool MEAS>
 static int launch_force_t(yk_ctx* c)
 {
@@ -441,19 +449,26 @@ static int launch_force_t(yk_ctx* c)
             c->pos, c->posf, c->perm, c->aii, c->fa, c->a, c->fpart, c->err);
         return 1;
     }
-    static int grid = 0, grid_near = 0;
+    static int grid = 0, grid_near = 0, grid_lo = 0;
     if (grid == 0) {
-        int per_sm = 0, per_sm_near = 0, sms = 0;
+        int per_sm = 0, per_sm_near = 0, per_sm_lo = 0, sms = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs<SIM, PREC, MEAS>, PB, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_near, k_force_near<SIM, PREC, MEAS>, PB, 0);
+        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lo, k_force_pairs<SIM, PREC, MEAS, true>, PB, 0);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
         grid = std::max(1, per_sm) * std::max(1, sms);
         grid_near = std::max(1, per_sm_near) * std::max(1, sms);
+        grid_lo = std::max(1, per_sm_lo) * std::max(1, sms);
     }
     cudaMemsetAsync(c->job_counter, 0, sizeof(int), c->stream);
     if (c->kernel == 3) {
         k_force_near<SIM, PREC, MEAS><<<std::min(grid_near, c->pj.njobs), PB, 0, c->stream>>>(
             c->pos, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+    } else if (lo_path<SIM, PREC>(c->fa)) {
+        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
+            k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid_lo, c->pj.njobs), PB, 0, c->stream>>>(
+                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
     } else {
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
             c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
@@ -1460,16 +1475,25 @@ static void noalloc_force(cudaStream_t st, const double4* pos, const float* posf
                           const ForceArgs& fa, double* Si, double* Sj, double* Sm, unsigned* err,
                           const int* perm, const double* zii, const double* aii, double* a)
 {
-    static int grid = 0;
+    static int grid = 0, grid_lo = 0;
     if (grid == 0) {
-        int per_sm = 0, sms = 0, dev = 0;
+        int per_sm = 0, per_sm_lo = 0, sms = 0, dev = 0;
         cudaGetDevice(&dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs<SIM, PREC, MEAS>, PB, 0);
+        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lo, k_force_pairs<SIM, PREC, MEAS, true>, PB, 0);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         grid = std::max(1, per_sm) * std::max(1, sms);
+        grid_lo = std::max(1, per_sm_lo) * std::max(1, sms);
     }
-    k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter, fa, Si, Sj,
-                                                                            Sm, err);
+    if (lo_path<SIM, PREC>(fa)) {
+        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
+            k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid_lo, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter,
+                                                                                      fa, Si, Sj, Sm, err);
+    } else {
+        k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter, fa, Si,
+                                                                                Sj, Sm, err);
+    }
     k_combine<SIM><<<(fa.n + 255) / 256, 256, 0, st>>>(Si, Sj, pj, perm, zii, aii, fa, a);
 }
 

@@ -43,6 +43,12 @@ namespace yk {
 constexpr int PB = 128;           // slots per block / tile (= threads per CTA)
 constexpr int PWARPS = PB / 32;
 
+// Type of the per-warp reaction rows: a row entry is one reduce-scatter
+// result, FP64 in the FP64 form and FP32 in the mixed form, so either type
+// holds it exactly.
+template <int PREC>
+using row_t = std::conditional_t<PREC == PREC_FP64, double, float>;
+
 struct PairJobs {
     const int2* jobs;             // (R, s) per job, costliest first
     int njobs;
@@ -128,7 +134,7 @@ template <int SIM, int PREC, bool MEAS, bool CHECK>
 __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& pi, const ScreenI& si,
                                            real_t<PREC> wi, const double4* tl, const float* tlf,
                                            int j0, int jlim, bool diag, bool active, int tid,
-                                           int sw, TargetAcc<PREC, MEAS>& acc, double* my_acc)
+                                           int sw, TargetAcc<PREC, MEAS>& acc, row_t<PREC>* my_acc)
 {
     using R_t = real_t<PREC>;
     const int g = j0 >> 2;
@@ -205,9 +211,9 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
         if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
             // a warp visits each group of a tile once, so this is the row
             // entry's only write (rows start at zero for skipped groups)
-            my_acc[3 * jl] = -(double)t[0];
-            my_acc[3 * jl + 1] = -(double)t[1];
-            my_acc[3 * jl + 2] = -(double)t[2];
+            my_acc[3 * jl] = -t[0];
+            my_acc[3 * jl + 1] = -t[1];
+            my_acc[3 * jl + 2] = -t[2];
         }
     }
 }
@@ -221,7 +227,7 @@ template <int SIM, bool MEAS, bool CHECK>
 __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
                                               float wi, const float* tlf, const float* tll, int j0, int jlim,
                                               bool diag, bool active, int tid, int sw,
-                                              TargetAcc<PREC_MIXED, MEAS>& acc, double* my_acc)
+                                              TargetAcc<PREC_MIXED, MEAS>& acc, float* my_acc)
 {
     const int g = j0 >> 2;
     float2 da[3], db[3];
@@ -290,9 +296,9 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
     if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
         // a warp visits each group of a tile once, so this is the row
         // entry's only write (rows start at zero for skipped groups)
-        my_acc[3 * jl] = (double)t[0];
-        my_acc[3 * jl + 1] = (double)t[1];
-        my_acc[3 * jl + 2] = (double)t[2];
+        my_acc[3 * jl] = t[0];
+        my_acc[3 * jl + 1] = t[1];
+        my_acc[3 * jl + 2] = t[2];
     }
 }
 
@@ -400,11 +406,12 @@ __device__ __forceinline__ unsigned near_groups(const ForceArgs& fa, const WarpB
     return gm;
 }
 
-// Shared memory of the half-pair kernels.
+// Shared memory of the half-pair kernels (RowT: row_t of the form).
+template <typename RowT>
 struct PairSmem {
     double4 tile[2][PB];                  // FP64 source tiles, or the shadow lo parts (TMA)
     float tilef[2][SHADOW_HI_FLOATS];     // FP32 shadow source tiles, hi parts and w (TMA)
-    double acc_j[2][PWARPS][PB * 3];      // per-warp reaction rows, one set per tile stage
+    RowT acc_j[2][PWARPS][PB * 3];        // per-warp reaction rows, one set per tile stage
     double red[32 * NSCAL];               // block reduction scratch
     uint64_t bar[2];                      // one mbarrier per tile stage
     int done[2];                          // warps finished with the stage's tile
@@ -422,7 +429,8 @@ struct BoxView {
     int n, M, seg, nseg_max;
 };
 
-__device__ __forceinline__ void pairs_smem_init(PairSmem& sm)
+template <typename RowT>
+__device__ __forceinline__ void pairs_smem_init(PairSmem<RowT>& sm)
 {
     // The ion path evaluates all 4 pairs of a group and masks the terms
     // (ion_pair_nb), so it also reads the slots of a partial tile that no copy
@@ -444,7 +452,8 @@ static_assert(SHADOW_LO_FLOATS * sizeof(float) <= PB * sizeof(double4), "lo part
 
 // Load source tile C of box bx into stage qq & 1 (one thread): the shadow hi
 // parts, and the FP64 positions or (lo) the shadow lo parts.
-__device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int C, unsigned qq, bool lo)
+template <typename RowT>
+__device__ __forceinline__ void pairs_issue(PairSmem<RowT>& sm, const BoxView& bx, int C, unsigned qq, bool lo)
 {
     const int j0 = C * PB;
     const int cnt = min(PB, bx.n - j0);
@@ -473,8 +482,12 @@ __device__ __forceinline__ void pairs_issue(PairSmem& sm, const BoxView& bx, int
 // only after that copy has landed, so it never overwrites rows that are
 // still being summed.  Warps may thus run up to one tile apart, which absorbs
 // the uneven work of the four target groups.
-template <int SIM, int PREC, bool MEAS>
-__device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, const BoxView& bx, int R, int sg,
+// LOMODE: whether the mixed ion path takes its displacement from the shadow's
+// hi/lo parts (pair_group_lo): 0 never, 1 always (the caller has checked
+// fa.lo; the FP64-tile path is then not compiled in, which frees its
+// registers), 2 as fa.lo says (boxes of a batch differ).
+template <int SIM, int PREC, bool MEAS, int LOMODE = 2>
+__device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const ForceArgs& fa, const BoxView& bx, int R, int sg,
                                           double* __restrict__ sm_row, unsigned* __restrict__ err,
                                           unsigned& q)
 {
@@ -496,7 +509,8 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
     acc.zero();
     // mixed-form ions on a box that allows it: FP32 displacements from the
     // shadow's hi/lo parts, no FP64 source tiles
-    const bool lo = (PREC == PREC_MIXED) && (SIM == SIM_PURE || SIM == SIM_MIX) && fa.lo != 0;
+    const bool lo = (PREC == PREC_MIXED) && (SIM == SIM_PURE || SIM == SIM_MIX) &&
+                    (LOMODE == 1 || (LOMODE == 2 && fa.lo != 0));
     float nli[3] = {0.f, 0.f, 0.f};
     if (lo) {
 #pragma unroll
@@ -517,7 +531,7 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
         const bool diag = (C == R);
         const double4* tl = sm.tile[st];
         const float* tlf = sm.tilef[st];
-        double* my_acc = sm.acc_j[st][warp];
+        row_t<PREC>* my_acc = sm.acc_j[st][warp];
 #pragma unroll
         for (int k = lane; k < PB * 3; k += 32) my_acc[k] = 0.0;
         __syncwarp();
@@ -583,13 +597,21 @@ __device__ __forceinline__ bool pairs_job(PairSmem& sm, const ForceArgs& fa, con
     return true;
 }
 
-template <int SIM, int PREC, bool MEAS>
-__global__ void __launch_bounds__(PB, 5)
+// Resident CTAs per SM: 5 (96 registers); the mixed kernel that always takes
+// the hi/lo displacement needs fewer registers and FP32 rows, so 6 fit.
+template <int PREC, bool LO>
+constexpr int pairs_ctas_per_sm()
+{
+    return (PREC == PREC_MIXED && LO) ? 6 : 5;
+}
+
+template <int SIM, int PREC, bool MEAS, bool LO = false>
+__global__ void __launch_bounds__(PB, (pairs_ctas_per_sm<PREC, LO>()))
 k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, PairJobs pj,
               int* __restrict__ job_counter, ForceArgs fa, double* __restrict__ Si,
               double* __restrict__ Sj, double* __restrict__ Sm, unsigned* __restrict__ err)
 {
-    __shared__ __align__(128) PairSmem sm;
+    __shared__ __align__(128) PairSmem<row_t<PREC>> sm;
     pairs_smem_init(sm);
     BoxView bx;
     bx.pos = pos;
@@ -607,7 +629,8 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
         const int job = sm.s_job;
         if (job >= pj.njobs) break;
         const int2 js = pj.jobs[job];
-        if (!pairs_job<SIM, PREC, MEAS>(sm, fa, bx, js.x, js.y, Sm + (size_t)job * NSCAL, err, q)) return;
+        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 0>(sm, fa, bx, js.x, js.y, Sm + (size_t)job * NSCAL, err, q))
+            return;
     }
 }
 

@@ -38,11 +38,12 @@ PB = 128
 
 def footprint_bytes(n, seg=8):
     """Device bytes a box of n particles holds inside a batch: state and
-    slot arrays (~260 B per particle) plus the half-pair scratch."""
+    slot arrays (~260 B per particle; 84 B per slot: FP64 positions and the
+    FP32 shadow) plus the half-pair scratch."""
     t = (n + PB - 1) // PB
     nseg = (t + seg - 1) // seg
     scratch = 8 * 3 * PB * (t * (t + 1) // 2 + t * nseg)
-    return 260 * n + 60 * PB * t + scratch + 4096
+    return 260 * n + 84 * PB * t + scratch + 4096
 
 
 @dataclass
