@@ -103,7 +103,7 @@ __device__ __forceinline__ bool near_job(NearSmem& sm, const ForceArgs& fa, cons
     const bool active = i < n;
     const double4 pi = active ? bx.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
     const R_t wi = (SIM == SIM_MIX) ? (R_t)pi.w : (R_t)1;   // Z_i of the reaction
-    const WarpBox box = warp_box(pi, active);
+    const WarpBox box = warp_box(fa, pi, active);
     const unsigned lt_mask = (1u << lane) - 1u;
     const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
     TargetAcc<PREC, MEAS> acc;

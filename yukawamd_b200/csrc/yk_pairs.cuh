@@ -312,6 +312,7 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
 // reach; the other groups skip even the per-pair FP32 screen.
 struct WarpBox {
     float lo[3], hi[3];
+    float c[3], h[3];                // centre and half-width plus the rounding margin
     bool any, has_p;                 // any active target; any proton target (nucleons)
 };
 
@@ -329,7 +330,7 @@ __device__ __forceinline__ float warp_maxf(float v)
     return v;
 }
 
-__device__ __forceinline__ WarpBox warp_box(const double4& pi, bool active)
+__device__ __forceinline__ WarpBox warp_box(const ForceArgs& fa, const double4& pi, bool active)
 {
     WarpBox b;
     const float inf = __int_as_float(0x7f800000);
@@ -339,30 +340,32 @@ __device__ __forceinline__ WarpBox warp_box(const double4& pi, bool active)
         const float v = __double2float_rn(c[k]);
         b.lo[k] = warp_minf(active ? v : inf);
         b.hi[k] = warp_maxf(active ? v : -inf);
+        // margin: 2^-18 L for the FP32 arithmetic (the box, its centre and
+        // the source's minimum image are each a few roundings of values below
+        // L) plus 2 SHADOW_Q for the grid rounding of the shadow coordinate
+        const float mu = fmaf(3.814697265625e-6f, fa.Lf[k], (float)(2.0 * SHADOW_Q));
+        b.c[k] = 0.5f * (b.lo[k] + b.hi[k]);
+        b.h[k] = fmaf(0.5f, b.hi[k] - b.lo[k], mu);
     }
     b.any = __any_sync(0xffffffffu, active);
     b.has_p = __any_sync(0xffffffffu, active && pi.w == 1.0);
     return b;
 }
 
-// Lower bound of the minimum-image distance^2 from source (x, w) to the box.
+// Lower bound of the minimum-image distance^2 from source (x, w) to the box:
+// per axis, the minimum image of x - c, less the half-width.  The images of
+// the box interval all have the same width, so the nearest is the one whose
+// centre is nearest; a box at least L wide gives 0.
 template <int SIM>
 __device__ __forceinline__ bool box_reaches(const ForceArgs& fa, const WarpBox& b, const float (&x)[3], float w)
 {
+    const float MAGIC = 12582912.0f;
     float dist2 = 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float L = fa.Lf[k];
-        // 2^-18 L for the FP32 arithmetic, plus 2 SHADOW_Q for the grid
-        // rounding of the shadow coordinate
-        const float mu = fmaf(3.814697265625e-6f, L, (float)(2.0 * SHADOW_Q));
-        const float lo = (b.lo[k] - x[k]) - mu;                  // x_i - x_j over the box
-        const float hi = (b.hi[k] - x[k]) + mu;
-        // distance from 0 to [lo, hi] + s L, the smallest over s = -1, 0, 1
-        const float m0 = fmaxf(0.f, fmaxf(lo, -hi));
-        const float m1 = fmaxf(0.f, fmaxf(lo - L, L - hi));
-        const float m2 = fmaxf(0.f, fmaxf(lo + L, -L - hi));
-        const float m = fminf(m0, fminf(m1, m2));
+        const float d = x[k] - b.c[k];
+        const float dm = fmaf(-fa.Lf[k], fmaf(d, fa.invLf[k], MAGIC) - MAGIC, d);
+        const float m = fmaxf(fabsf(dm) - b.h[k], 0.f);
         dist2 = fmaf(m, m, dist2);
     }
     float lim;
@@ -504,7 +507,7 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
     const R_t wi = (SIM == SIM_MIX) ? (R_t)pi.w : (R_t)1;   // Z_i of the reaction
     const bool all_active = (R + 1) * PB <= n;
     const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
-    const WarpBox box = warp_box(pi, active);
+    const WarpBox box = warp_box(fa, pi, active);
     TargetAcc<PREC, MEAS> acc;
     acc.zero();
     // mixed-form ions on a box that allows it: FP32 displacements from the
