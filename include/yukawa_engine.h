@@ -265,8 +265,8 @@ typedef struct yk_tuning {
                              3 half-pair kernel over per-warp near-source lists;
                              yk_get_tuning reports the kernel auto resolved to */
     int pair_seg;         /* source tiles per job of the half-pair kernels;
-                             0 = automatic (8, shorter for small boxes so that
-                             every resident CTA gets at least two jobs)       */
+                             0 = automatic (about M / 130 for M tiles of 128
+                             slots, at least 1)                               */
     int sort_every;       /* steps between Hilbert re-orderings (-1 = never)  */
     int graph_steps;      /* steps captured per CUDA graph by yk_run          */
 } yk_tuning;

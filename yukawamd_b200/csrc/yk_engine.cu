@@ -322,26 +322,16 @@ static void free_pairs(yk_ctx* c)
 
 // Build the job table of the half-pair kernel (costliest jobs first) and its
 // scratch.  Unused Sj / Si slots are never read.
-// Jobs of the half-pair kernels for M tiles cut into runs of seg tiles.
-static long long pair_job_count(int M, int seg)
-{
-    long long k = 0;
-    for (int R = 0; R < M; ++R) k += (M - R + seg - 1) / seg;
-    return k;
-}
-
 static int setup_pairs(yk_ctx* c)
 {
     free_pairs(c);
     const int M = (c->n + PB - 1) / PB;
     if (c->seg_auto) {
-        // The longest job bounds the force call: keep at least two jobs per
-        // resident CTA (5 per SM), cutting runs shorter for small boxes.
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
-        int seg = DEFAULT_SEG;
-        while (seg > 1 && pair_job_count(M, seg) < 2LL * 5 * sms) seg >>= 1;
-        c->seg = seg;
+        // Shorter jobs balance the persistent CTAs' tails better; longer ones
+        // write and combine fewer target-side partials.  Measured on a B200
+        // (force call, seg 1..8): best seg 1 at M = 32 and 128 tiles, 2-3 at
+        // M = 400-432, 6-8 at M = 1024, i.e. about M / 130 (about 65 M jobs).
+        c->seg = std::min(32, std::max(1, (M + 65) / 130));
     }
     const int seg = c->seg;
     std::vector<int2> jobs;
