@@ -264,9 +264,9 @@ typedef struct yk_tuning {
                              2 half-pair kernel (Newton's third law, scratch),
                              3 half-pair kernel over per-warp near-source lists;
                              yk_get_tuning reports the kernel auto resolved to */
-    int pair_seg;         /* source tiles per job of the half-pair kernels;
-                             0 = automatic (about M / 130 for M tiles of 128
-                             slots, at least 1)                               */
+    int pair_seg;         /* longest job of the half-pair kernels, in source
+                             tiles (jobs shrink towards the end of the job
+                             list); 0 = automatic (8 FP64, 4 mixed)         */
     int sort_every;       /* steps between Hilbert re-orderings (-1 = never)  */
     int graph_steps;      /* steps captured per CUDA graph by yk_run          */
 } yk_tuning;

@@ -193,9 +193,9 @@ k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ p
         bx.Sj = Sj + d->Sj_off;
         bx.n = sfa.n;
         bx.M = d->T;
-        bx.seg = d->seg;
         bx.nseg_max = d->nseg;
-        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 2>(sm, sfa, bx, jb.y, jb.z,
+        const int C0 = jb.y + jb.z * d->seg;
+        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 2>(sm, sfa, bx, jb.y, C0, min(C0 + d->seg, bx.M), jb.z,
                                                     Sm + (size_t)(d->sm_off + jb.w) * NSCAL, err, q))
             return;
     }

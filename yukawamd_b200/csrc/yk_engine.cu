@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -58,7 +59,13 @@ __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b)
 // Largest scratch the half-pair kernel may take before auto mode falls back
 // to the scratch-free row kernel.
 constexpr size_t PAIR_SCRATCH_BUDGET = size_t(8) << 30;
-constexpr int DEFAULT_SEG = 8;
+// Longest job of the half-pair kernels (tiles) when the caller leaves it to
+// the engine.  Measured on a B200 (force call, guided job sizes, caps 4..64):
+// FP64 is best at 8 from N = 4,096 to 131,072; the mixed form at 4 for N =
+// 16,384 to 55,296 and 8 at 131,072 (within 1.5 % of 4).
+constexpr int DEFAULT_SEG_FP64 = 8;
+constexpr int DEFAULT_SEG_MIXED = 4;
+constexpr int DEFAULT_SEG = DEFAULT_SEG_FP64;
 constexpr int DEFAULT_SORT_EVERY = 50;
 constexpr int DEFAULT_GRAPH_STEPS = 50;
 constexpr int MAX_GRAPHS = 8;
@@ -100,7 +107,8 @@ struct yk_ctx {
     unsigned* h_err = nullptr;
     // half-pair kernel
     double *Si = nullptr, *Sj = nullptr, *Sm = nullptr;
-    int2* jobs = nullptr;
+    int4* jobs = nullptr;
+    int* row_slots = nullptr;
     int* job_counter = nullptr;
     PairJobs pj{};
     // argument blocks and tunables
@@ -111,7 +119,7 @@ struct yk_ctx {
     int kernel = 2;                 // 1 rows, 2 pairs, 3 near lists (resolved, never 0)
     int kernel_req = 0;             // as requested (0 = auto)
     int seg = DEFAULT_SEG;
-    bool seg_auto = true;           // pair_seg not set by the caller: pick it from N
+    bool seg_auto = true;           // pair_seg not set by the caller: the precision's default
     int sort_every = DEFAULT_SORT_EVERY;
     int graph_steps = DEFAULT_GRAPH_STEPS;
     long long step_count = 0;       // integrator steps since create
@@ -299,14 +307,59 @@ static void drop_graphs(yk_ctx* c)
 }
 
 // Scratch bytes of the half-pair kernel for n particles and segment length.
-static size_t pair_scratch_bytes(int n, int seg)
+// Jobs of the half-pair kernel for M tiles, in dispatch order (costliest
+// first), by guided self-scheduling: each job takes
+//     d = clamp(W / (2 P), 1, smax)
+// tiles from the start of the row with the most tiles left, W being the work
+// not yet handed out and P the number of resident CTAs.  The bulk of the work
+// goes out in long jobs (few target-side partials to write and combine, few
+// job prologues), and the sizes shrink towards the end so that the persistent
+// CTAs finish together.  row_slots[R] counts the Si slots of row R.
+static void build_pair_jobs(int M, int smax, int P, std::vector<int4>& jobs, std::vector<int>& row_slots)
 {
-    const size_t M = (size_t)(n + PB - 1) / PB;
-    const size_t nseg = (M + seg - 1) / seg;
-    const size_t units = M * (M + 1) / 2;
-    size_t jobs = 0;
-    for (size_t R = 0; R < M; ++R) jobs += (M - R + seg - 1) / seg;
-    return sizeof(double) * (units * PB * 3 + M * nseg * PB * 3 + jobs * NSCAL) + sizeof(int2) * jobs;
+    jobs.clear();
+    row_slots.assign(M, 0);
+    std::vector<int> done(M, 0);
+    long long W = (long long)M * (M + 1) / 2;
+    std::priority_queue<std::pair<int, int>> rows;          // (tiles left, -R): longest row, then lowest R
+    for (int R = 0; R < M; ++R) rows.push(std::make_pair(M - R, -R));
+    while (!rows.empty()) {
+        const int left = rows.top().first, R = -rows.top().second;
+        rows.pop();
+        const long long want = W / (2LL * std::max(P, 1));
+        const int d = (int)std::min<long long>(left, std::min<long long>(smax, std::max<long long>(1, want)));
+        const int C0 = R + done[R];
+        jobs.push_back(make_int4(R, C0, C0 + d, row_slots[R]++));
+        done[R] += d;
+        W -= d;
+        if (left > d) rows.push(std::make_pair(left - d, -R));
+    }
+}
+
+static int auto_pair_seg(const yk_ctx* c)
+{
+    return c->p.precision == YK_PREC_MIXED ? DEFAULT_SEG_MIXED : DEFAULT_SEG_FP64;
+}
+
+// Resident CTAs of the half-pair kernels on a device (the most any variant
+// runs per SM), for the job builder.
+static int pair_ctas(int dev)
+{
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return 6 * sms;
+}
+
+static size_t pair_scratch_bytes(int n, int seg, int dev)
+{
+    const int M = (n + PB - 1) / PB;
+    std::vector<int4> jobs;
+    std::vector<int> slots;
+    build_pair_jobs(M, seg, pair_ctas(dev), jobs, slots);
+    const size_t nseg = M > 0 ? (size_t)*std::max_element(slots.begin(), slots.end()) : 0;
+    const size_t units = (size_t)M * (M + 1) / 2;
+    return sizeof(double) * (units * PB * 3 + (size_t)M * nseg * PB * 3 + jobs.size() * NSCAL) +
+           sizeof(int4) * jobs.size() + sizeof(int) * (size_t)M;
 }
 
 static void free_pairs(yk_ctx* c)
@@ -317,49 +370,34 @@ static void free_pairs(yk_ctx* c)
     cudaFree(c->jobs);
     c->Si = c->Sj = c->Sm = nullptr;
     c->jobs = nullptr;
+    cudaFree(c->row_slots);
+    c->row_slots = nullptr;
     c->pj = PairJobs{};
 }
 
-// Build the job table of the half-pair kernel (costliest jobs first) and its
+// Build the job table of the half-pair kernel (build_pair_jobs) and its
 // scratch.  Unused Sj / Si slots are never read.
 static int setup_pairs(yk_ctx* c)
 {
     free_pairs(c);
     const int M = (c->n + PB - 1) / PB;
-    if (c->seg_auto) {
-        // Shorter jobs balance the persistent CTAs' tails better; longer ones
-        // write and combine fewer target-side partials.  Measured on a B200
-        // (force call, seg 1..8): best seg 1 at M = 32 and 128 tiles, 2-3 at
-        // M = 400-432, 6-8 at M = 1024, i.e. about M / 130 (about 65 M jobs).
-        c->seg = std::min(32, std::max(1, (M + 65) / 130));
-    }
-    const int seg = c->seg;
-    std::vector<int2> jobs;
-    std::vector<int> cost;
-    for (int R = 0; R < M; ++R) {
-        const int L = M - R;
-        for (int s = 0; s * seg < L; ++s) {
-            jobs.push_back(make_int2(R, s));
-            const int tiles = std::min(seg, L - s * seg);
-            cost.push_back(2 * tiles - (s == 0 ? 1 : 0));   // diagonal tile ~ half
-        }
-    }
-    std::vector<int> order(jobs.size());
-    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
-    std::stable_sort(order.begin(), order.end(), [&](int u, int w) { return cost[u] > cost[w]; });
-    std::vector<int2> sorted(jobs.size());
-    for (size_t k = 0; k < order.size(); ++k) sorted[k] = jobs[order[k]];
-    const int nseg = (M + seg - 1) / seg;
+    if (c->seg_auto) c->seg = auto_pair_seg(c);
+    std::vector<int4> jobs;
+    std::vector<int> slots;
+    build_pair_jobs(M, c->seg, pair_ctas(c->dev), jobs, slots);
+    const int nseg = M > 0 ? *std::max_element(slots.begin(), slots.end()) : 0;
     const size_t units = (size_t)M * (M + 1) / 2;
     CK(c, cudaMalloc((void**)&c->Sj, sizeof(double) * units * PB * 3));
     CK(c, cudaMalloc((void**)&c->Si, sizeof(double) * (size_t)M * nseg * PB * 3));
-    CK(c, cudaMalloc((void**)&c->Sm, sizeof(double) * sorted.size() * NSCAL));
-    CK(c, cudaMalloc((void**)&c->jobs, sizeof(int2) * sorted.size()));
-    CK(c, cudaMemcpy(c->jobs, sorted.data(), sizeof(int2) * sorted.size(), cudaMemcpyHostToDevice));
+    CK(c, cudaMalloc((void**)&c->Sm, sizeof(double) * jobs.size() * NSCAL));
+    CK(c, cudaMalloc((void**)&c->jobs, sizeof(int4) * jobs.size()));
+    CK(c, cudaMalloc((void**)&c->row_slots, sizeof(int) * (size_t)std::max(M, 1)));
+    CK(c, cudaMemcpy(c->jobs, jobs.data(), sizeof(int4) * jobs.size(), cudaMemcpyHostToDevice));
+    CK(c, cudaMemcpy(c->row_slots, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice));
     c->pj.jobs = c->jobs;
-    c->pj.njobs = (int)sorted.size();
+    c->pj.row_slots = c->row_slots;
+    c->pj.njobs = (int)jobs.size();
     c->pj.M = M;
-    c->pj.seg = seg;
     c->pj.nseg_max = nseg;
     return YK_OK;
 }
@@ -372,7 +410,7 @@ static int resolve_kernel(yk_ctx* c)
     // autotuner candidate: with nucleons in species-major slot order it is
     // 1.35x slower than kernel 2 on the 51,200-nucleon box, and on the
     // 55,296-ion mixture 1.5x slower.)
-    if (k == 0) k = (pair_scratch_bytes(c->n, c->seg) <= PAIR_SCRATCH_BUDGET) ? 2 : 1;
+    if (k == 0) k = (pair_scratch_bytes(c->n, c->seg, c->dev) <= PAIR_SCRATCH_BUDGET) ? 2 : 1;
     if (k == 2 || k == 3) {
         int rc = setup_pairs(c);
         if (rc) return rc;
@@ -799,6 +837,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
         return fail(nullptr, YK_ERR_CUDA, "cudaSetDevice(%d) failed", p->device);
     }
     setup_args(c);
+    c->seg = auto_pair_seg(c);
 
     // HBM admission: refuse up front rather than fail half-way.
     size_t cub_bytes = 0;
@@ -807,8 +846,9 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
                    (sizeof(double4) + sizeof(float) * SHADOW_FLOATS / SHADOW_TILE) * ((size_t)n + SHADOW_TILE) + sizeof(int) * 5 * (size_t)n + cub_bytes +
                    sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;
-    const bool pairs_fit = pair_scratch_bytes(n, c->seg) <= PAIR_SCRATCH_BUDGET;
-    if (pairs_fit) bytes += pair_scratch_bytes(n, c->seg);
+    const size_t pair_bytes = pair_scratch_bytes(n, c->seg, c->dev);
+    const bool pairs_fit = pair_bytes <= PAIR_SCRATCH_BUDGET;
+    if (pairs_fit) bytes += pair_bytes;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         delete c;
@@ -922,7 +962,7 @@ int yk_set_tuning(yk_ctx* c, const yk_tuning* t)
     drop_graphs(c);
     c->kernel_req = t->force_kernel;
     c->seg_auto = t->pair_seg <= 0;
-    c->seg = t->pair_seg > 0 ? t->pair_seg : DEFAULT_SEG;
+    c->seg = t->pair_seg > 0 ? t->pair_seg : auto_pair_seg(c);
     const int old_sort = c->sort_every;
     c->sort_every = t->sort_every == 0 ? DEFAULT_SORT_EVERY : t->sort_every;
     c->graph_steps = t->graph_steps > 0 ? t->graph_steps : DEFAULT_GRAPH_STEPS;
@@ -1415,20 +1455,23 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 static void* g_noalloc_addr[NOALLOC_MAX_DEVICES];
 static std::mutex g_noalloc_mutex;
 
-__global__ void k_noalloc_prepare(int* perm, int n, int2* jobs, int M, int seg)
+__global__ void k_noalloc_prepare(int* perm, int n, int4* jobs, int* row_slots, int M, int seg)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < n) perm[s] = s;                      // slots in the caller's order
     if (s == 0) {
         int k = 0;
-        for (int R = 0; R < M; ++R)
-            for (int q = 0; q * seg < M - R; ++q) jobs[k++] = make_int2(R, q);
+        for (int R = 0; R < M; ++R) {
+            int q = 0;
+            for (; q * seg < M - R; ++q) jobs[k++] = make_int4(R, R + q * seg, min(R + (q + 1) * seg, M), q);
+            row_slots[R] = q;
+        }
     }
 }
 
 // Byte layout of the scratch for n particles (256-byte aligned pieces).
 struct NoallocLayout {
-    size_t pos, posf, perm, iperm, Si, Sj, Sm, jobs, ds, counter, err, total;
+    size_t pos, posf, perm, iperm, Si, Sj, Sm, jobs, row_slots, ds, counter, err, total;
     int M, nseg, njobs;
 };
 
@@ -1452,7 +1495,8 @@ static NoallocLayout noalloc_layout(int n)
     L.Si = take(sizeof(double) * 3 * PB * (size_t)L.M * L.nseg);
     L.Sj = take(sizeof(double) * 3 * PB * ((size_t)L.M * (L.M + 1) / 2));
     L.Sm = take(sizeof(double) * NSCAL * (size_t)L.njobs);
-    L.jobs = take(sizeof(int2) * (size_t)L.njobs);
+    L.jobs = take(sizeof(int4) * (size_t)L.njobs);
+    L.row_slots = take(sizeof(int) * (size_t)L.M);
     L.ds = take(sizeof(DevScalars));
     L.counter = take(sizeof(int));
     L.err = take(sizeof(unsigned));
@@ -1547,7 +1591,8 @@ extern "C" int yk_accel_noalloc(const yk_params* p, int n, const double* x_dev, 
     double* Si = reinterpret_cast<double*>(b + L.Si);
     double* Sj = reinterpret_cast<double*>(b + L.Sj);
     double* Sm = reinterpret_cast<double*>(b + L.Sm);
-    int2* jobs = reinterpret_cast<int2*>(b + L.jobs);
+    int4* jobs = reinterpret_cast<int4*>(b + L.jobs);
+    int* row_slots = reinterpret_cast<int*>(b + L.row_slots);
     DevScalars* ds = reinterpret_cast<DevScalars*>(b + L.ds);
     int* counter = reinterpret_cast<int*>(b + L.counter);
     unsigned* err = reinterpret_cast<unsigned*>(b + L.err);
@@ -1566,7 +1611,7 @@ extern "C" int yk_accel_noalloc(const yk_params* p, int n, const double* x_dev, 
     CK(nullptr, cudaMemsetAsync(ds, 0, sizeof(DevScalars), st));
     CK(nullptr, cudaMemsetAsync(counter, 0, sizeof(int), st));
     CK(nullptr, cudaMemsetAsync(err, 0, sizeof(unsigned), st));
-    k_noalloc_prepare<<<(n + 255) / 256, 256, 0, st>>>(perm, n, jobs, L.M, NOALLOC_SEG);
+    k_noalloc_prepare<<<(n + 255) / 256, 256, 0, st>>>(perm, n, jobs, row_slots, L.M, NOALLOC_SEG);
     k_apply_perm<<<(n + VBLOCK - 1) / VBLOCK, VBLOCK, 0, st>>>(perm, iperm, x_dev, zii_dev, pos, posf, n,
                                                               tmp.sa.pack_w);
     int k = 2;
@@ -1574,7 +1619,7 @@ extern "C" int yk_accel_noalloc(const yk_params* p, int n, const double* x_dev, 
     pj.jobs = jobs;
     pj.njobs = L.njobs;
     pj.M = L.M;
-    pj.seg = NOALLOC_SEG;
+    pj.row_slots = row_slots;
     pj.nseg_max = L.nseg;
     const bool mixed = p->precision == YK_PREC_MIXED;
     switch (p->sim_type) {

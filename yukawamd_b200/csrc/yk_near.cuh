@@ -90,15 +90,15 @@ __device__ __forceinline__ bool near_classify(const ForceArgs& fa, const WarpBox
 }
 
 template <int SIM, int PREC, bool MEAS>
-__device__ __forceinline__ bool near_job(NearSmem& sm, const ForceArgs& fa, const BoxView& bx, int R, int sg,
+__device__ __forceinline__ bool near_job(NearSmem& sm, const ForceArgs& fa, const BoxView& bx, int R, int C0, int C1,
+                                         int sg,
                                          double* __restrict__ sm_row, unsigned* __restrict__ err, unsigned& q)
 {
     using R_t = real_t<PREC>;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int n = bx.n;
-    const int C0 = R + sg * bx.seg;
-    const int C1 = min(C0 + bx.seg, bx.M);
+
     const int i = R * PB + tid;
     const bool active = i < n;
     const double4 pi = active ? bx.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
@@ -280,7 +280,6 @@ k_force_near(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ job
     bx.Sj = Sj;
     bx.n = fa.n;
     bx.M = pj.M;
-    bx.seg = pj.seg;
     bx.nseg_max = pj.nseg_max;
     unsigned q = 0;
     for (;;) {
@@ -288,8 +287,9 @@ k_force_near(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ job
         __syncthreads();
         const int job = sm.s_job;
         if (job >= pj.njobs) break;
-        const int2 js = pj.jobs[job];
-        if (!near_job<SIM, PREC, MEAS>(sm, fa, bx, js.x, js.y, Sm + (size_t)job * NSCAL, err, q)) return;
+        const int4 js = pj.jobs[job];
+        if (!near_job<SIM, PREC, MEAS>(sm, fa, bx, js.x, js.y, js.z, js.w, Sm + (size_t)job * NSCAL, err, q))
+            return;
     }
 }
 

@@ -50,11 +50,13 @@ template <int PREC>
 using row_t = std::conditional_t<PREC == PREC_FP64, double, float>;
 
 struct PairJobs {
-    const int2* jobs;             // (R, s) per job, costliest first
+    const int4* jobs;             // (R, C0, C1, slot) per job, costliest first:
+                                  // target block R, source tiles C0 <= C < C1,
+                                  // Si slot of row R that the job writes
+    const int* row_slots;         // Si slots written per row R
     int njobs;
     int M;                        // tiles
-    int seg;                      // source tiles per job
-    int nseg_max;                 // ceil(M / seg): Si slots per row
+    int nseg_max;                 // Si slots per row in the layout (max of row_slots)
 };
 
 __host__ __device__ __forceinline__ long long tri_index(int C, int R)
@@ -429,7 +431,7 @@ struct BoxView {
     const float* posf;
     double* Si;
     double* Sj;
-    int n, M, seg, nseg_max;
+    int n, M, nseg_max;
 };
 
 template <typename RowT>
@@ -490,16 +492,14 @@ __device__ __forceinline__ void pairs_issue(PairSmem<RowT>& sm, const BoxView& b
 // fa.lo; the FP64-tile path is then not compiled in, which frees its
 // registers), 2 as fa.lo says (boxes of a batch differ).
 template <int SIM, int PREC, bool MEAS, int LOMODE = 2>
-__device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const ForceArgs& fa, const BoxView& bx, int R, int sg,
-                                          double* __restrict__ sm_row, unsigned* __restrict__ err,
-                                          unsigned& q)
+__device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const ForceArgs& fa, const BoxView& bx, int R,
+                                          int C0, int C1, int sg, double* __restrict__ sm_row,
+                                          unsigned* __restrict__ err, unsigned& q)
 {
     using R_t = real_t<PREC>;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int n = bx.n;
-    const int C0 = R + sg * bx.seg;
-    const int C1 = min(C0 + bx.seg, bx.M);
     const int i = R * PB + tid;
     const bool active = i < n;
     const double4 pi = active ? bx.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
@@ -623,7 +623,6 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
     bx.Sj = Sj;
     bx.n = fa.n;
     bx.M = pj.M;
-    bx.seg = pj.seg;
     bx.nseg_max = pj.nseg_max;
     unsigned q = 0;
     for (;;) {
@@ -631,8 +630,9 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
         __syncthreads();
         const int job = sm.s_job;
         if (job >= pj.njobs) break;
-        const int2 js = pj.jobs[job];
-        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 0>(sm, fa, bx, js.x, js.y, Sm + (size_t)job * NSCAL, err, q))
+        const int4 js = pj.jobs[job];
+        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 0>(sm, fa, bx, js.x, js.y, js.z, js.w, Sm + (size_t)job * NSCAL,
+                                                    err, q))
             return;
     }
 }
@@ -649,7 +649,7 @@ k_combine(const double* __restrict__ Si, const double* __restrict__ Sj, PairJobs
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= fa.n) return;
     const int R = p / PB, l = p % PB;
-    const int nseg = (pj.M - R + pj.seg - 1) / pj.seg;
+    const int nseg = pj.row_slots[R];
     double F[3] = {0.0, 0.0, 0.0};
     const double* si = Si + ((size_t)R * pj.nseg_max * PB + l) * 3;
     for (int s = 0; s < nseg; ++s) {
