@@ -353,6 +353,8 @@ static int pair_ctas(int dev)
 static size_t pair_scratch_bytes(int n, int seg, int dev)
 {
     const int M = (n + PB - 1) / PB;
+    const size_t sj_bytes = sizeof(double) * ((size_t)M * (M + 1) / 2) * PB * 3;
+    if (sj_bytes > PAIR_SCRATCH_BUDGET) return sj_bytes;       // too large anyway: skip the job list
     std::vector<int4> jobs;
     std::vector<int> slots;
     build_pair_jobs(M, seg, pair_ctas(dev), jobs, slots);
