@@ -503,7 +503,7 @@ static int launch_force_t(yk_ctx* c)
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
             c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
     }
-    k_combine<SIM><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->Si, c->Sj, c->pj, c->perm, c->zii,
+    k_combine<SIM><<<c->pj.M, COMB_THREADS, 0, c->stream>>>(c->Si, c->Sj, c->pj, c->perm, c->zii,
                                                               c->aii, c->fa, c->a);
     return 2;
 }
@@ -1530,7 +1530,7 @@ static void noalloc_force(cudaStream_t st, const double4* pos, const float* posf
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter, fa, Si,
                                                                                 Sj, Sm, err);
     }
-    k_combine<SIM><<<(fa.n + 255) / 256, 256, 0, st>>>(Si, Sj, pj, perm, zii, aii, fa, a);
+    k_combine<SIM><<<pj.M, COMB_THREADS, 0, st>>>(Si, Sj, pj, perm, zii, aii, fa, a);
 }
 
 template <int SIM>

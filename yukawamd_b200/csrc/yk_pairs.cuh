@@ -30,9 +30,9 @@
 //   Si[R][s][PB][3]       target-side sums of job (R, s)
 //   Sj[tri(C,R)][PB][3]   source-side sums of unit (R, C), tri(C,R) = C(C+1)/2+R
 //   Sm[job][8]            measurement sums of the job (U, W, P tensor)
-// k_combine adds, for every slot, its Si entries then its Sj entries in a
-// fixed order, applies the reference's scaling and scatters to the caller's
-// particle order.  Results are therefore bit-reproducible, independent of
+// k_combine adds, for every slot, its Si and Sj entries in a fixed order
+// (two interleaved groups, then the group sums), applies the reference's
+// scaling and scatters to the caller's particle order.  Results are therefore bit-reproducible, independent of
 // which CTA ran which job.
 #pragma once
 
@@ -639,34 +639,50 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
 
 // Per slot: sum its target-side and source-side partials in a fixed order,
 // scale (int_ion_pure.f:227-231 / int_ion_mix.f:201,273-277 / int_nn.f:318-322)
-// and store into the caller's order.
+// and store into the caller's order.  One CTA per target block R (the
+// heaviest blocks, with the most units, first); thread t of each of the
+// COMB_GROUPS groups owns double t of the block's 128 x 3 partial rows (slot
+// t / 3, component t % 3), so a warp reads 256 contiguous bytes per row.
+// Group g sums the rows g, g + COMB_GROUPS, ...; the group sums are added
+// in group order.  The summation order is fixed, so results are
+// bit-reproducible run to run.
+constexpr int COMB_GROUPS = 2;
+constexpr int COMB_THREADS = COMB_GROUPS * PB * 3;
+
 template <int SIM>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(COMB_THREADS)
 k_combine(const double* __restrict__ Si, const double* __restrict__ Sj, PairJobs pj,
           const int* __restrict__ perm, const double* __restrict__ zii,
           const double* __restrict__ aii, ForceArgs fa, double* __restrict__ a_out)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= fa.n) return;
-    const int R = p / PB, l = p % PB;
+    __shared__ double part[COMB_GROUPS][PB * 3];
+    const int R = pj.M - 1 - (int)blockIdx.x;
+    const int g = threadIdx.x / (PB * 3), t = threadIdx.x % (PB * 3);
+    constexpr size_t ROW = (size_t)PB * 3;
+    double F = 0.0;
+    const double* si = Si + (size_t)R * pj.nseg_max * ROW + t;
     const int nseg = pj.row_slots[R];
-    double F[3] = {0.0, 0.0, 0.0};
-    const double* si = Si + ((size_t)R * pj.nseg_max * PB + l) * 3;
-    for (int s = 0; s < nseg; ++s) {
-        const double* e = si + (size_t)s * PB * 3;
-        F[0] += e[0];
-        F[1] += e[1];
-        F[2] += e[2];
+#pragma unroll 4
+    for (int s = g; s < nseg; s += COMB_GROUPS) F += si[(size_t)s * ROW];
+    const double* sj = Sj + (size_t)tri_index(R, 0) * ROW + t;
+#pragma unroll 4
+    for (int R2 = g; R2 <= R; R2 += COMB_GROUPS) F += sj[(size_t)R2 * ROW];
+    part[g][t] = F;
+    __syncthreads();
+    const int l = threadIdx.x;
+    const int p = R * PB + l;
+    if (l < PB && p < fa.n) {
+        double Fv[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double v = part[0][3 * l + c];
+#pragma unroll
+            for (int q = 1; q < COMB_GROUPS; ++q) v += part[q][3 * l + c];
+            Fv[c] = v;
+        }
+        const int orig = perm[p];
+        store_accel<SIM>(fa, orig, zii[orig], aii, Fv, a_out);
     }
-    const double* sj = Sj + ((size_t)tri_index(R, 0) * PB + l) * 3;
-    for (int R2 = 0; R2 <= R; ++R2) {
-        const double* e = sj + (size_t)R2 * PB * 3;
-        F[0] += e[0];
-        F[1] += e[1];
-        F[2] += e[2];
-    }
-    const int orig = perm[p];
-    store_accel<SIM>(fa, orig, zii[orig], aii, F, a_out);
 }
 
 }  // namespace yk
