@@ -8,8 +8,11 @@
 //                         sums in registers) against source tile C (one 1-D
 //                         TMA bulk copy into shared memory, double-buffered).
 //                         On the diagonal unit only pairs j > i count.
-//   job  (R, s)         : units C = R + s*seg ... of one row; persistent CTAs
-//                         pull jobs from an atomic counter (costliest first).
+//   job  (R, C0, C1, s) : units C0 <= C < C1 of row R, writing Si slot s of
+//                         the row; persistent CTAs pull jobs from an atomic
+//                         counter in the order of the job table (long jobs
+//                         first, shrinking towards the end: the engine's
+//                         build_pair_jobs).
 //
 // Reaction sums: each warp sweeps the whole tile in groups of 4 sources.  In
 // step jj of a group, lane L takes source jj ^ sw(L), sw(L) = 2*bit4(L) +
@@ -17,23 +20,25 @@
 // 0, and the slots that a halving exchange sends are the same for every lane
 // (slots 2,3 over xor 16, then slot 1 over xor 8): the warp sums the 32
 // lanes' reactions on the 4 sources with that reduce-scatter plus a 3-level
-// butterfly (36 shuffles per group instead of 4 x 30, no selects), in FP64
-// for both forms, and lanes 0/8/16/24 add the four sums to the warp's own
-// accumulator row in shared memory.  The 4 warp rows are added in a fixed
-// order at the end of the tile, so no atomics and no per-phase barriers.
-// Every pair is first tested on FP32 shadow positions, two sources per packed
-// FP32x2 instruction (screen_r2_x2); a group none of whose 128 pairs can be
-// inside a cutoff is skipped, and only candidates take the exact FP64
-// minimum-image test and the physics.
+// butterfly (18 shuffles of 3-vector components per group instead of 4 x 15,
+// no selects; FP64 in the FP64 form, FP32 in the mixed form), and lanes
+// 0/8/16/24 write the four sums into the warp's own row in shared memory.
+// The 4 warp rows are added in a fixed order at the end of the tile by the
+// warp that finishes it last, so no atomics and no per-tile block barrier.
+// A warp first skips the 4-source groups that cannot reach the bounding box
+// of its targets (near_groups); the others are screened per pair on the FP32
+// shadow positions, two sources per packed FP32x2 instruction, and only groups
+// with a candidate take the pair terms (pair_group; pair_group_lo for the
+// mixed form's ions).
 //
 // Outputs are partial sums in scratch (nothing is accumulated atomically):
-//   Si[R][s][PB][3]       target-side sums of job (R, s)
+//   Si[R][s][PB][3]       target-side sums of job (R, ., ., s)
 //   Sj[tri(C,R)][PB][3]   source-side sums of unit (R, C), tri(C,R) = C(C+1)/2+R
 //   Sm[job][8]            measurement sums of the job (U, W, P tensor)
 // k_combine adds, for every slot, its Si and Sj entries in a fixed order
 // (two interleaved groups, then the group sums), applies the reference's
-// scaling and scatters to the caller's particle order.  Results are therefore bit-reproducible, independent of
-// which CTA ran which job.
+// scaling and scatters to the caller's particle order.  Results are
+// therefore bit-reproducible, independent of which CTA ran which job.
 #pragma once
 
 #include "yk_force.cuh"
