@@ -2,7 +2,8 @@
 
 For one box the engine can run its force call two ways (the half-pair kernel
 with scratch, or the row kernel that evaluates each pair from both sides)
-and cut the half-pair work into jobs of `pair_seg` source tiles; it refreshes
+and cap the half-pair jobs at `pair_seg` source tiles (the job list shrinks
+them towards its end); it refreshes
 the Morton order every `sort_every` steps.  Which choice is fastest depends on
 N, the cutoff radius relative to the box, the interaction and the precision,
 so the tuner measures candidates on the caller's own workload (CUDA-event
