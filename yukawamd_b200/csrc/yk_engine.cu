@@ -499,6 +499,10 @@ static int launch_force_t(yk_ctx* c)
         if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
             k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid_lo, c->pj.njobs), PB, 0, c->stream>>>(
                 c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+    } else if (SIM != SIM_NUCLEON && c->fa.img_k) {
+        if constexpr (SIM != SIM_NUCLEON)
+            k_force_pairs<SIM, PREC, MEAS, false, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
+                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
     } else {
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
             c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);

@@ -406,19 +406,23 @@ __device__ __forceinline__ void pair32(const ForceArgs& fa, const double4& pi, c
 // the image integer k, so the reference's d - L (d > L/2) or d + L
 // (d < -L/2) is d + k L, one FMA, when k is exact (fa.img_k, see the host
 // setup); otherwise the conditional corrections themselves.
+// IMGK: the caller has checked fa.img_k (the exact comparisons are then not
+// compiled in).
+template <bool IMGK = false>
 __device__ __forceinline__ double image_k(const ForceArgs& fa, double d, float k, int c)
 {
+    if (IMGK) return __fma_rn((double)k, fa.xl[c], d);
     return fa.img_k ? __fma_rn((double)k, fa.xl[c], d) : min_image(d, fa.xl[c], fa.hlb[c]);
 }
 
-template <int PREC, bool MEAS>
+template <int PREC, bool MEAS, bool IMGK = false>
 __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& pi, const double4& pj, bool sel,
                                             const float (&k)[3],
                                             PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o)
 {
-    const double dx = image_k(fa, __dsub_rn(pi.x, pj.x), k[0], 0);
-    const double dy = image_k(fa, __dsub_rn(pi.y, pj.y), k[1], 1);
-    const double dz = image_k(fa, __dsub_rn(pi.z, pj.z), k[2], 2);
+    const double dx = image_k<IMGK>(fa, __dsub_rn(pi.x, pj.x), k[0], 0);
+    const double dy = image_k<IMGK>(fa, __dsub_rn(pi.y, pj.y), k[1], 1);
+    const double dz = image_k<IMGK>(fa, __dsub_rn(pi.z, pj.z), k[2], 2);
     if constexpr (PREC == PREC_FP64) {
         o.dx = dx;
         o.dy = dy;

@@ -137,7 +137,7 @@ __device__ __forceinline__ void reduce_scatter4(T (&r)[4][3], T (&t)[3])
 // one at 2 (sw ^ 2)), so each step's image integers are plain registers.
 // CHECK: the tile is partial, diagonal, or the CTA has inactive targets, so
 // every pair needs the validity test.
-template <int SIM, int PREC, bool MEAS, bool CHECK>
+template <int SIM, int PREC, bool MEAS, bool CHECK, bool IMGK = false>
 __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& pi, const ScreenI& si,
                                            real_t<PREC> wi, const double4* tl, const float* tlf,
                                            int j0, int jlim, bool diag, bool active, int tid,
@@ -178,7 +178,7 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
                                 jj == 0 ? ka[1].x : jj == 1 ? ka[1].y : jj == 2 ? kb[1].x : kb[1].y,
                                 jj == 0 ? ka[2].x : jj == 1 ? ka[2].y : jj == 2 ? kb[2].x : kb[2].y};
             PairOut<R_t> o;
-            ion_pair_nb<PREC, MEAS>(fa, pi, pjv, ((m >> jj) & 1u) != 0, k, o);
+            ion_pair_nb<PREC, MEAS, IMGK>(fa, pi, pjv, ((m >> jj) & 1u) != 0, k, o);
             if constexpr (PREC == PREC_FP64) acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
             else gs.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
             const R_t fsj = o.fs * wi;               // 0 unless the pair interacts
@@ -496,7 +496,7 @@ __device__ __forceinline__ void pairs_issue(PairSmem<RowT>& sm, const BoxView& b
 // hi/lo parts (pair_group_lo): 0 never, 1 always (the caller has checked
 // fa.lo; the FP64-tile path is then not compiled in, which frees its
 // registers), 2 as fa.lo says (boxes of a batch differ).
-template <int SIM, int PREC, bool MEAS, int LOMODE = 2>
+template <int SIM, int PREC, bool MEAS, int LOMODE = 2, bool IMGK = false>
 __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const ForceArgs& fa, const BoxView& bx, int R,
                                           int C0, int C1, int sg, double* __restrict__ sm_row,
                                           unsigned* __restrict__ err, unsigned& q)
@@ -560,11 +560,11 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
             }
         } else if (!diag && jlim == PB && all_active) {
             for (; gm; gm &= gm - 1)
-                pair_group<SIM, PREC, MEAS, false>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
+                pair_group<SIM, PREC, MEAS, false, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
                                                    active, tid, sw, acc, my_acc);
         } else {
             for (; gm; gm &= gm - 1)
-                pair_group<SIM, PREC, MEAS, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
+                pair_group<SIM, PREC, MEAS, true, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
                                                   active, tid, sw, acc, my_acc);
         }
         // this warp is done with the tile: the last warp reduces and refills
@@ -613,7 +613,10 @@ constexpr int pairs_ctas_per_sm()
     return (PREC == PREC_MIXED && LO) ? 6 : 5;
 }
 
-template <int SIM, int PREC, bool MEAS, bool LO = false>
+// LO: the mixed ion kernel for boxes with fa.lo (pair_group_lo); IMGK: a
+// kernel for ion boxes with fa.img_k (the screen's image integers replace the
+// exact minimum-image comparisons, which are then not compiled in).
+template <int SIM, int PREC, bool MEAS, bool LO = false, bool IMGK = false>
 __global__ void __launch_bounds__(PB, (pairs_ctas_per_sm<PREC, LO>()))
 k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, PairJobs pj,
               int* __restrict__ job_counter, ForceArgs fa, double* __restrict__ Si,
@@ -636,8 +639,8 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
         const int job = sm.s_job;
         if (job >= pj.njobs) break;
         const int4 js = pj.jobs[job];
-        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 0>(sm, fa, bx, js.x, js.y, js.z, js.w, Sm + (size_t)job * NSCAL,
-                                                    err, q))
+        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 0, IMGK>(sm, fa, bx, js.x, js.y, js.z, js.w,
+                                                          Sm + (size_t)job * NSCAL, err, q))
             return;
     }
 }
