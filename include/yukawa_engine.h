@@ -309,6 +309,17 @@ YK_API int yk_perf_read(yk_ctx* ctx, yk_perf* out);
  * over the whole GPU.  Used for roofline denominators. */
 YK_API int yk_peak_probe(int device, int kind, double* tflops);
 
+/* The half-pair kernel's job table for m tiles of 128 slots, as yk_create
+ * builds it: jobs of at most cap source tiles, in dispatch order, sized by
+ * guided self-scheduling for ctas resident CTAs.  A job is four ints
+ * (R, C0, C1, slot): target block R, source tiles C0 <= C < C1 (C0 >= R),
+ * and the slot of row R's target-side partial that it writes.  Writes at
+ * most max_jobs jobs to jobs (NULL: only count) and the m slot counts to
+ * row_slots (NULL allowed); returns the number of jobs, or -YK_ERR_ARG.
+ * Host arithmetic only (no GPU), for inspecting and testing the schedule.
+ * No counterpart in the reference. */
+YK_API long long yk_pair_jobs(int m, int cap, int ctas, int* jobs, long long max_jobs, int* row_slots);
+
 /*
  * Force call that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory when

@@ -54,6 +54,8 @@ SIGNATURES = {
     "yk_perf_enable": (C.c_int, [_ctx, C.c_int, C.c_size_t]),
     "yk_perf_read": (C.c_int, [_ctx, C.POINTER(abi.YkPerf)]),
     "yk_peak_probe": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "yk_pair_jobs": (C.c_longlong, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_longlong,
+                                    C.POINTER(C.c_int)]),
     "yk_accel_noalloc": (C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p, _S, C.c_void_p]),
     "yk_host_register": (C.c_int, [C.c_void_p, C.c_size_t]),

@@ -754,6 +754,24 @@ extern "C" {
 
 const char* yk_version(void) { return YK_VERSION_STR; }
 
+long long yk_pair_jobs(int m, int cap, int ctas, int* jobs, long long max_jobs, int* row_slots)
+{
+    if (m < 1 || cap < 1 || ctas < 1 || max_jobs < 0 || (jobs == nullptr && max_jobs > 0))
+        return -(long long)YK_ERR_ARG;
+    std::vector<int4> list;
+    std::vector<int> slots;
+    build_pair_jobs(m, cap, ctas, list, slots);
+    const long long k = std::min<long long>(max_jobs, (long long)list.size());
+    for (long long j = 0; j < k; ++j) {
+        jobs[4 * j] = list[j].x;
+        jobs[4 * j + 1] = list[j].y;
+        jobs[4 * j + 2] = list[j].z;
+        jobs[4 * j + 3] = list[j].w;
+    }
+    if (row_slots) std::copy(slots.begin(), slots.end(), row_slots);
+    return (long long)list.size();
+}
+
 unsigned long long yk_kernel_launch_count(void) { return g_launches.load(); }
 
 int yk_params_default(yk_params* p)

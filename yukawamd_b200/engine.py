@@ -315,6 +315,21 @@ def peak_probe(device=0, kind=0):
     return out.value
 
 
+def pair_jobs(m, cap, ctas):
+    """The half-pair kernel's job table for m tiles (yk_pair_jobs): an int
+    array of shape (jobs, 4) with rows (R, C0, C1, slot) in dispatch order,
+    and the Si slot count of every row.  Host arithmetic only."""
+    k = lib().yk_pair_jobs(int(m), int(cap), int(ctas), None, 0, None)
+    if k < 0:
+        raise ValueError("yk_pair_jobs: bad arguments (m=%r, cap=%r, ctas=%r)" % (m, cap, ctas))
+    jobs = np.zeros((k, 4), dtype=np.int32)
+    slots = np.zeros(int(m), dtype=np.int32)
+    got = lib().yk_pair_jobs(int(m), int(cap), int(ctas), jobs.ctypes.data_as(C.POINTER(C.c_int)), k,
+                             slots.ctypes.data_as(C.POINTER(C.c_int)))
+    assert got == k
+    return jobs, slots
+
+
 def accel_noalloc(params, n, x_dev, zii_dev, aii_dev, do_measurements, a_dev, stream=None):
     """Force call on caller-owned device arrays (raw device addresses as ints)
     that allocates no device memory; see yk_accel_noalloc in
