@@ -15,8 +15,9 @@ by barriers and the time is the max over ranks.  Rank 0 prints one JSON line.
 
 --impl reference times the reference's CPU algorithm, i.e. the OpenMP C
 restatement in oracle/ (the Fortran cannot be compiled on these machines), on
-all host cores, each step one force call over a bounded block of target rows
-of the same full-size box.
+all host cores, each step one whole force call over the same full-size box
+(or, on hosts too slow for that, a block of target rows centred on the middle
+row, which has the whole call's mean row length).
 """
 import argparse
 import json
@@ -322,48 +323,67 @@ def read_traffic(kind, precision):
     return None
 
 
+def _pairs_of_rows(n, r0, r1):
+    """Unique pairs of target rows r0 <= i < r1 (row i pairs with j > i)."""
+    r1 = min(r1, n - 1)
+    if r1 <= r0:
+        return 0
+    return (r1 - r0) * (n - 1) - (r0 + r1 - 1) * (r1 - r0) // 2
+
+
+def cpu_rows(n, rate, budget_s):
+    """Target rows for one timed CPU call: all of them when a whole force
+    call fits budget_s at `rate` pairs/s, else a block centred on the middle
+    row.  The reference's loop costs a per-row part (its omp for / omp single
+    barriers, int_ion_mix.f:159-213) plus a part proportional to the row's
+    n-1-i pairs; a centred block has the whole call's mean row length, so
+    both parts weigh as in a whole call."""
+    total = n * (n - 1) // 2
+    if total <= budget_s * rate:
+        return 0, n, "whole force calls over"
+    # rows of mean length (n-1)/2 cost about (n-1)/2 pairs each
+    nrows = int(min(n - 2, max(64, 2.0 * budget_s * rate / (n - 1))))
+    r0 = max(0, (n - nrows) // 2)
+    return r0, r0 + nrows, "target rows %d..%d (centred on the middle row) of" % (r0, r0 + nrows)
+
+
+def _calibrate(orc, p, w):
+    """pairs/s of the oracle's OpenMP loop on a small centred block."""
+    n = w.n
+    r0 = max(0, n // 2 - 32)
+    orc.set_row_range(r0, r0 + 64)
+    t0 = time.perf_counter()
+    orc.accel(p, w.x, w.zii, w.aii, False)
+    dt = time.perf_counter() - t0
+    orc.set_row_range()
+    return _pairs_of_rows(n, r0, r0 + 64) / max(dt, 1e-6)
+
+
 def cpu_sample(w, kind, target_s=12.0):
     """Time the oracle's OpenMP force loop (reference structure) on all host
-    cores over a block of target rows of the full-size box."""
+    cores: whole force calls repeated to about target_s, or one centred block
+    of target rows when a whole call takes longer."""
     from oracle.oracle import Oracle
     cores = os.cpu_count() or 1
     orc = Oracle("double", threads=cores)
     p = w.yk_params()
     n = w.n
-    mid = n // 2
-
-    def run(nrows):
-        orc.set_row_range(mid, mid + nrows)
-        t0 = time.perf_counter()
+    rate = _calibrate(orc, p, w)
+    r0, r1, what = cpu_rows(n, rate, target_s)
+    pairs1 = _pairs_of_rows(n, r0, r1)
+    reps = max(1, int(round(target_s * rate / max(pairs1, 1))))
+    orc.set_row_range(r0, r1)
+    t0 = time.perf_counter()
+    for _ in range(reps):
         orc.accel(p, w.x, w.zii, w.aii, False)
-        dt = time.perf_counter() - t0
-        pairs = sum(n - 1 - i for i in range(mid, min(mid + nrows, n - 1)))
-        return dt, pairs
-
-    dt, pairs = run(64)                                   # calibration
-    rate = pairs / max(dt, 1e-6)
-    total = n * (n - 1) // 2
-    if target_s * rate < total / 2:
-        # less than half a force call: a block of target rows from the middle
-        nrows = int(min(n // 2 - 1, max(64, target_s * rate / (n - mid))))
-        dt, pairs = run(nrows)
-        what = "target rows %d..%d of" % (mid, mid + nrows)
-    else:
-        # whole force calls, repeated to about target_s
-        reps = max(1, int(round(target_s * rate / total)))
-        orc.set_row_range()
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            orc.accel(p, w.x, w.zii, w.aii, False)
-        dt = time.perf_counter() - t0
-        pairs = reps * total
-        what = "%d complete force calls over" % reps
+    dt = time.perf_counter() - t0
     orc.set_row_range()
+    pairs = reps * pairs1
     return {"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": "force-only calls of the oracle's OpenMP loop (%s structure, OMP_SCHEDULE=%s): "
-                      "%s the full N=%d box, %d pairs in %.2f s"
+                      "%d calls, %s the full N=%d box, %d pairs in %.2f s"
                       % ({"mix": "int_ion_mix.f", "ocp": "int_ion_pure.f"}.get(kind, "int_nn.f"),
-                         os.environ.get("OMP_SCHEDULE", "static"), what, n, pairs, dt)}
+                         os.environ.get("OMP_SCHEDULE", "static"), reps, what, n, pairs, dt)}
 
 
 def run_ours(args, dist):
@@ -591,18 +611,12 @@ def run_reference(args):
     p = w.yk_params()
     cores = os.cpu_count() or 1
     orc = Oracle("double", threads=cores)
-    mid = n // 2
-
-    def pairs_of(r0, r1):
-        return sum(n - 1 - i for i in range(r0, min(r1, n - 1)))
-
-    # size each step to ~3 s of CPU work so the whole run stays within minutes
-    orc.set_row_range(mid, mid + 64)
-    t0 = time.perf_counter()
-    orc.accel(p, w.x, w.zii, w.aii, False)
-    rate = pairs_of(mid, mid + 64) / max(time.perf_counter() - t0, 1e-6)
-    nrows = int(min(n // 2 - 1, max(64, 3.0 * rate / (n - mid))))
-    orc.set_row_range(mid, mid + nrows)
+    # each step is one force call over whole box when that takes <= 4 s on
+    # these cores, else over a centred block of rows of about 4 s, so the
+    # whole --steps K --warmup W run stays within minutes
+    rate = _calibrate(orc, p, w)
+    r0, r1, what = cpu_rows(n, rate, 4.0)
+    orc.set_row_range(r0, r1)
     for _ in range(args.warmup):
         orc.accel(p, w.x, w.zii, w.aii, False)
     times = []
@@ -611,12 +625,12 @@ def run_reference(args):
         orc.accel(p, w.x, w.zii, w.aii, False)
         times.append(time.perf_counter() - t0)
     orc.set_row_range()
-    pairs = pairs_of(mid, mid + nrows)
+    pairs = _pairs_of_rows(n, r0, r1)
     total = sum(times)
     value = pairs * args.steps / total
     sample = ("each step: one force-only call of the oracle's OpenMP loop (reference "
-              "structure: omp for over j per target i, omp single fold) over target rows "
-              "%d..%d of the full N=%d box = %d pairs" % (mid, mid + nrows, n, pairs))
+              "structure: omp for over j per target i, omp single fold; OMP_SCHEDULE=%s) over %s "
+              "the full N=%d box = %d pairs" % (os.environ.get("OMP_SCHEDULE", "static"), what, n, pairs))
     return {"metric": BASELINE_METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,

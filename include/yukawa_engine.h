@@ -323,9 +323,10 @@ YK_API long long yk_pair_jobs(int m, int cap, int ctas, int* jobs, long long max
 /*
  * Force call that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory when
- * they need forces -- code running while a stream is captured into a CUDA
- * graph (cudaMalloc is not allowed there) or applications whose own pool
- * allocator owns all device memory.  It computes what yk_accel computes, for
+ * they need forces -- applications whose own pool allocator owns all device
+ * memory, and callers that cannot afford the device-wide synchronisation of
+ * cudaFree / cudaMalloc on their other streams.  It computes what yk_accel
+ * computes, for
  * one box given entirely by caller-owned DEVICE arrays: x_dev double[3n],
  * zii_dev / aii_dev double[n] (NULL allowed where yk_create allows NULL),
  * a_dev double[3(n+3)] (output, same layout as yk_accel's a_out).  out (host)
@@ -342,6 +343,18 @@ YK_API int yk_accel_noalloc(const yk_params* p, int n,
                             const double* x_dev, const double* zii_dev,
                             const double* aii_dev, int do_meas,
                             double* a_dev, yk_scalars* out, void* stream);
+
+/* Failure-path check of the device-side waits.  The reference has no device
+ * and no error codes (a fatal error calls md_exit, md_utils.f:158-183); the
+ * engine's kernels instead bound every wait on a tile copy and report
+ * YK_ERR_TIMEOUT.  This launches one CTA on ctx's stream that waits, with
+ * both of the kernels' wait forms limited to `spins` polls (1 .. 2^22), on a
+ * barrier that no copy ever completes, so every wait gives up.  Returns
+ * YK_ERR_TIMEOUT through the same error word and check as yk_accel, clears
+ * it, and leaves the context usable; *gave_up (may be NULL) receives the
+ * number of threads that gave up (128).  Any other return is a failure of
+ * the check itself. */
+YK_API int yk_wait_selftest(yk_ctx* ctx, long long spins, int* gave_up);
 
 /* Page-lock a caller-owned host buffer so that yk_get_state / yk_set_state
  * copy it by DMA.  Optional. */

@@ -58,6 +58,7 @@ SIGNATURES = {
                                     C.POINTER(C.c_int)]),
     "yk_accel_noalloc": (C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p, _S, C.c_void_p]),
+    "yk_wait_selftest": (C.c_int, [_ctx, C.c_longlong, C.POINTER(C.c_int)]),
     "yk_host_register": (C.c_int, [C.c_void_p, C.c_size_t]),
     "yk_host_unregister": (C.c_int, [C.c_void_p]),
     "yk_kernel_launch_count": (C.c_ulonglong, []),

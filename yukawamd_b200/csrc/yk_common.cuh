@@ -73,11 +73,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
     return ok != 0;
 }
 
-// Wait for phase `parity` of *bar with at most SPIN_LIMIT polls.  Returns
+// Wait for phase `parity` of *bar with at most `limit` polls.  Returns
 // false (and sets ERR_TIMEOUT in *err) if the phase never completed.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* err)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* err,
+                                                  long long limit = SPIN_LIMIT)
 {
-    for (long long it = 0; it < SPIN_LIMIT; ++it)
+    for (long long it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     atomicOr(err, ERR_TIMEOUT);
     return false;
@@ -87,9 +88,9 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
 // barrier between waits: a waiter also gives up as soon as another thread has
 // raised *abort, and one that times out raises it.
 __device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, unsigned parity, unsigned* err,
-                                                    volatile int* abort)
+                                                    volatile int* abort, long long limit = SPIN_LIMIT)
 {
-    for (long long it = 0; it < SPIN_LIMIT; ++it) {
+    for (long long it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((it & 63) == 63 && *abort) return false;
     }

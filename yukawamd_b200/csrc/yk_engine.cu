@@ -56,6 +56,34 @@ __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b)
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Failure path of the bounded waits (yk_wait_selftest): one CTA of 128
+// threads waits on an mbarrier that no copy is ever issued against, so its
+// phase 0 never completes.  Warps 0-1 wait as the pair kernels' warps do
+// (mbar_wait_abortable: the first to give up raises the abort flag, the
+// others then leave), warps 2-3 as the row kernel does (mbar_wait_bounded).
+// Every wait ends after at most `spins` polls and sets ERR_TIMEOUT in *err;
+// nothing is in flight when the CTA exits.  out[0] counts the threads that
+// gave up (all 128 when the path works).
+__global__ void __launch_bounds__(128) k_wait_selftest(long long spins, unsigned* __restrict__ err,
+                                                       int* __restrict__ out)
+{
+    __shared__ uint64_t bar;
+    __shared__ int abort_flag;
+    __shared__ int gave_up;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        abort_flag = 0;
+        gave_up = 0;
+    }
+    __syncthreads();
+    const bool ok = threadIdx.x < 64 ? mbar_wait_abortable(&bar, 0u, err, &abort_flag, spins)
+                                     : mbar_wait_bounded(&bar, 0u, err, spins);
+    if (!ok) atomicAdd(&gave_up, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) out[0] = gave_up;
+}
+
 // Largest scratch the half-pair kernel may take before auto mode falls back
 // to the scratch-free row kernel.
 constexpr size_t PAIR_SCRATCH_BUDGET = size_t(8) << 30;
@@ -471,6 +499,27 @@ static bool lo_path(const ForceArgs& fa)
     return PREC == PREC_MIXED && SIM != SIM_NUCLEON && fa.lo != 0;
 }
 
+// Persistent grid of a PB-thread kernel on device dev (the current device):
+// resident CTAs per SM times the SM count.  Cached per (kernel, device); the
+// entries are atomics, so two first calls at once only repeat the query.
+constexpr int GRID_CACHE_DEVICES = 64;
+
+template <auto KERNEL>
+static int persistent_grid(int dev)
+{
+    static std::atomic<int> cache[GRID_CACHE_DEVICES];
+    const bool cached = dev >= 0 && dev < GRID_CACHE_DEVICES;
+    int g = cached ? cache[dev].load(std::memory_order_relaxed) : 0;
+    if (g == 0) {
+        int per_sm = 0, sms = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KERNEL, PB, 0);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = std::max(1, per_sm) * std::max(1, sms);
+        if (cached) cache[dev].store(g, std::memory_order_relaxed);
+    }
+    return g;
+}
+
 template <int SIM, int PREC, bool MEAS>
 static int launch_force_t(yk_ctx* c)
 {
@@ -479,31 +528,25 @@ static int launch_force_t(yk_ctx* c)
             c->pos, c->posf, c->perm, c->aii, c->fa, c->a, c->fpart, c->err);
         return 1;
     }
-    static int grid = 0, grid_near = 0, grid_lo = 0;
-    if (grid == 0) {
-        int per_sm = 0, per_sm_near = 0, per_sm_lo = 0, sms = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs<SIM, PREC, MEAS>, PB, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_near, k_force_near<SIM, PREC, MEAS>, PB, 0);
-        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lo, k_force_pairs<SIM, PREC, MEAS, true>, PB, 0);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
-        grid = std::max(1, per_sm) * std::max(1, sms);
-        grid_near = std::max(1, per_sm_near) * std::max(1, sms);
-        grid_lo = std::max(1, per_sm_lo) * std::max(1, sms);
-    }
     cudaMemsetAsync(c->job_counter, 0, sizeof(int), c->stream);
     if (c->kernel == 3) {
-        k_force_near<SIM, PREC, MEAS><<<std::min(grid_near, c->pj.njobs), PB, 0, c->stream>>>(
+        const int grid = persistent_grid<k_force_near<SIM, PREC, MEAS>>(c->dev);
+        k_force_near<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
             c->pos, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
     } else if (lo_path<SIM, PREC>(c->fa)) {
-        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
-            k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid_lo, c->pj.njobs), PB, 0, c->stream>>>(
+        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON) {
+            const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(c->dev);
+            k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
                 c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+        }
     } else if (SIM != SIM_NUCLEON && c->fa.img_k) {
-        if constexpr (SIM != SIM_NUCLEON)
+        if constexpr (SIM != SIM_NUCLEON) {
+            const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, false, true>>(c->dev);
             k_force_pairs<SIM, PREC, MEAS, false, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
                 c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+        }
     } else {
+        const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS>>(c->dev);
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
             c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
     }
@@ -1432,6 +1475,24 @@ int yk_peak_probe(int device, int kind, double* tflops)
     return YK_OK;
 }
 
+int yk_wait_selftest(yk_ctx* c, long long spins, int* gave_up)
+{
+    if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
+    if (spins < 1 || spins > SPIN_LIMIT)
+        return fail(c, YK_ERR_ARG, "spins must be in [1, %lld] (got %lld)", SPIN_LIMIT, spins);
+    CK(c, cudaSetDevice(c->dev));
+    // the count goes through the packed-scalar scratch of k_finish, which the
+    // next force call rewrites
+    int* dcount = reinterpret_cast<int*>(c->ds);
+    k_wait_selftest<<<1, 128, 0, c->stream>>>(spins, c->err, dcount);
+    g_launches += 1;
+    int h = -1;
+    CK(c, cudaMemcpyAsync(&h, dcount, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    const int rc = sync_and_check(c);
+    if (gave_up) *gave_up = h;
+    return rc;
+}
+
 int yk_host_register(void* ptr, size_t bytes)
 {
     if (!ptr || !bytes) return fail(nullptr, YK_ERR_ARG, "bad host buffer");
@@ -1454,13 +1515,15 @@ int yk_host_unregister(void* ptr)
 // Force call without device allocation (yk_accel_noalloc).
 //
 // Some callers cannot allocate device memory at the moment they need forces:
-// code that runs while a stream is being captured into a CUDA graph (where
-// cudaMalloc is not permitted), or applications that hand every byte of
-// device memory to their own pool allocator and forbid allocations behind
-// its back.  For them this entry point evaluates one force call on
-// caller-owned device arrays and keeps all of its working memory -- packed
-// positions, their FP32 shadow, the slot order, the job table and the
-// partial sums of the half-pair kernel -- in the file-scope array below.
+// applications that hand every byte of device memory to their own pool
+// allocator at start-up and forbid allocations behind its back, and callers
+// that cannot afford the device-wide synchronisation that cudaFree (and at
+// times cudaMalloc) imposes on every other stream of the GPU.  For them this
+// entry point evaluates one force call on caller-owned device arrays and keeps
+// all of its working memory -- packed positions, their FP32 shadow, the slot
+// order, the job table and the partial sums of the half-pair kernel -- in the
+// file-scope array below.  The call itself waits for its stream and copies
+// the scalars to the host before it returns.
 // The array is created when the library's device code is loaded and stays
 // on every GPU that loaded it until the process exits.  It caps n at
 // NOALLOC_MAX_N; larger calls are rejected.  All calls share the array: two
@@ -1529,26 +1592,18 @@ static NoallocLayout noalloc_layout(int n)
 }
 
 template <int SIM, int PREC, bool MEAS>
-static void noalloc_force(cudaStream_t st, const double4* pos, const float* posf, PairJobs pj, int* counter,
-                          const ForceArgs& fa, double* Si, double* Sj, double* Sm, unsigned* err,
+static void noalloc_force(int dev, cudaStream_t st, const double4* pos, const float* posf, PairJobs pj,
+                          int* counter, const ForceArgs& fa, double* Si, double* Sj, double* Sm, unsigned* err,
                           const int* perm, const double* zii, const double* aii, double* a)
 {
-    static int grid = 0, grid_lo = 0;
-    if (grid == 0) {
-        int per_sm = 0, per_sm_lo = 0, sms = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_pairs<SIM, PREC, MEAS>, PB, 0);
-        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lo, k_force_pairs<SIM, PREC, MEAS, true>, PB, 0);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        grid = std::max(1, per_sm) * std::max(1, sms);
-        grid_lo = std::max(1, per_sm_lo) * std::max(1, sms);
-    }
     if (lo_path<SIM, PREC>(fa)) {
-        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON)
-            k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid_lo, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter,
-                                                                                      fa, Si, Sj, Sm, err);
+        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON) {
+            const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(dev);
+            k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter,
+                                                                                   fa, Si, Sj, Sm, err);
+        }
     } else {
+        const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS>>(dev);
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter, fa, Si,
                                                                                 Sj, Sm, err);
     }
@@ -1556,17 +1611,17 @@ static void noalloc_force(cudaStream_t st, const double4* pos, const float* posf
 }
 
 template <int SIM>
-static void noalloc_force_s(bool mixed, bool meas, cudaStream_t st, const double4* pos, const float* posf,
-                            PairJobs pj, int* counter, const ForceArgs& fa, double* Si, double* Sj,
-                            double* Sm, unsigned* err, const int* perm, const double* zii,
+static void noalloc_force_s(bool mixed, bool meas, int dev, cudaStream_t st, const double4* pos,
+                            const float* posf, PairJobs pj, int* counter, const ForceArgs& fa, double* Si,
+                            double* Sj, double* Sm, unsigned* err, const int* perm, const double* zii,
                             const double* aii, double* a)
 {
     if (mixed) {
-        if (meas) noalloc_force<SIM, PREC_MIXED, true>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
-        else noalloc_force<SIM, PREC_MIXED, false>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+        if (meas) noalloc_force<SIM, PREC_MIXED, true>(dev, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+        else noalloc_force<SIM, PREC_MIXED, false>(dev, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
     } else {
-        if (meas) noalloc_force<SIM, PREC_FP64, true>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
-        else noalloc_force<SIM, PREC_FP64, false>(st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+        if (meas) noalloc_force<SIM, PREC_FP64, true>(dev, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
+        else noalloc_force<SIM, PREC_FP64, false>(dev, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii, aii, a);
     }
 }
 
@@ -1648,17 +1703,17 @@ extern "C" int yk_accel_noalloc(const yk_params* p, int n, const double* x_dev, 
     const bool mixed = p->precision == YK_PREC_MIXED;
     switch (p->sim_type) {
     case YK_SIM_PURE_ION:
-        noalloc_force_s<SIM_PURE>(mixed, meas, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii_dev,
+        noalloc_force_s<SIM_PURE>(mixed, meas, dev, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii_dev,
                                   aii_dev, a_dev);
         k += 2;
         break;
     case YK_SIM_ION_MIXTURE:
-        noalloc_force_s<SIM_MIX>(mixed, meas, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii_dev,
+        noalloc_force_s<SIM_MIX>(mixed, meas, dev, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm, zii_dev,
                                  aii_dev, a_dev);
         k += 2;
         break;
     case YK_SIM_NUCLEON:
-        noalloc_force_s<SIM_NUCLEON>(mixed, meas, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm,
+        noalloc_force_s<SIM_NUCLEON>(mixed, meas, dev, st, pos, posf, pj, counter, fa, Si, Sj, Sm, err, perm,
                                      zii_dev, aii_dev, a_dev);
         k += 2;
         break;

@@ -689,7 +689,8 @@ k_combine(const double* __restrict__ Si, const double* __restrict__ Sj, PairJobs
             Fv[c] = v;
         }
         const int orig = perm[p];
-        store_accel<SIM>(fa, orig, zii[orig], aii, Fv, a_out);
+        // only the mixture folds by Z_i; pure-ion and nucleon callers may pass zii = NULL
+        store_accel<SIM>(fa, orig, SIM == SIM_MIX ? zii[orig] : 0.0, aii, Fv, a_out);
     }
 }
 
