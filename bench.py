@@ -74,6 +74,12 @@ def parse():
     ap.add_argument("--drift-warmup", type=int, default=20,
                     help="warm-up groups of 100 steps (cancel_vcom + tnorm after each) before --drift")
     ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--line-drift-steps", type=int, default=10000,
+                    help="steps of the drift block of the default line (0: leave it out)")
+    ap.add_argument("--no-served", action="store_true",
+                    help="leave the served-ensemble block out of the default line")
+    ap.add_argument("--served-rate", type=float, default=64.0,
+                    help="Poisson arrival rate (runs/s) of the served ensemble in the default line")
     ap.add_argument("--serve", action="store_true",
                     help="instead of the benchmark: serve a request stream and report latency")
     ap.add_argument("--serve-ensemble", action="store_true",
@@ -456,10 +462,16 @@ def run_ours(args, dist):
                       "force_rms_rel_err_vs_fp64": ferr, "ev_rel_err": ev_err,
                       "px_rel_err": px_err}
         e2.close()
+        if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
+            out["mixed"]["vs_oracle"] = mixed_vs_oracle(w)
 
     if not args.no_extras and dist.world == 1:
         out["nucleon"] = nucleon_pair(K, W, me, dist)
         out["ensemble"] = ensemble(args.ensemble_steps, me, dist)
+        if args.line_drift_steps > 0:
+            out["drift"] = drift_block(w, kind, args.line_drift_steps, args.drift_warmup, dist)
+        if not args.no_served:
+            out["served"] = served_ensemble(args, dist)
 
     if not args.no_e2e:
         t_e2e, bi, bo = e2e_engine(w, K, W, me, dist)
@@ -473,6 +485,83 @@ def run_ours(args, dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_sample(w, kind)
     return out
+
+
+def mixed_vs_oracle(w):
+    """The mixed form's errors against one complete call of the FP64 CPU oracle
+    (int_ion_mix.f:105-295 restated, OpenMP on all host cores) on the same
+    positions: force 2-norm relative error, ev, px and pp."""
+    from oracle.oracle import Oracle
+    from yukawamd_b200 import abi
+    from yukawamd_b200.engine import Engine
+    orc = Oracle("double", threads=os.cpu_count() or 1)
+    p = w.yk_params()
+    n = w.n
+    t0 = time.perf_counter()
+    a_ref, s_ref = orc.accel(p, w.x, w.zii, w.aii, True)
+    t_orc = time.perf_counter() - t0
+    with Engine(w, precision=abi.YK_PREC_MIXED) as e:
+        s = e.accel(True)
+        a = e.a.copy()
+    return {"force_rms_rel_err": float(np.linalg.norm(a[:3 * n] - a_ref[:3 * n]) / np.linalg.norm(a_ref[:3 * n])),
+            "ev_rel_err": abs(s.ev - s_ref.ev) / abs(s_ref.ev),
+            "px_rel_err": abs(s.px - s_ref.px) / abs(s_ref.px),
+            "pp_rel_err": float(np.linalg.norm(np.array(s.pp) - np.array(s_ref.pp)) / np.linalg.norm(np.array(s_ref.pp))),
+            "oracle": "one measuring force call of the FP64 CPU oracle over all N(N-1)/2 pairs (%.1f s, %d threads)"
+                      % (t_orc, os.cpu_count() or 1)}
+
+
+def drift_block(w, kind, steps, warmup_groups, dist):
+    """Total-energy drift of the benchmark box over `steps` steps in FP64 and
+    in the mixed form, from one state equilibrated as md.F does (warm-up
+    groups of 100 FP64 steps, each followed by cancel_vcom and tnorm,
+    md.F:87-101); E = ev + ek per particle every 100 steps (the cadence of
+    md.F's energy record, md.F:125-157)."""
+    from yukawamd_b200 import abi
+    from yukawamd_b200.driver import RunControl, run_md
+    from yukawamd_b200.engine import Engine
+    out = {"workload": workload_desc(w, kind), "steps": steps, "every": 100,
+           "warmup": "%d groups x 100 FP64 steps with cancel_vcom + tnorm (md.F:87-101)" % warmup_groups}
+    x, v = w.x, w.v
+    t0 = time.perf_counter()
+    if warmup_groups > 0:
+        with Engine(w, device=dist.local, precision=abi.YK_PREC_FP64) as e:
+            run_md(e, RunControl(nwgroup=warmup_groups, nwsteps=100))
+            x, v, _vold, _a = e.get_state()
+    for prec in ("fp64", "mixed"):
+        yp = w.yk_params(precision=abi.YK_PREC_MIXED if prec == "mixed" else abi.YK_PREC_FP64)
+        with Engine(yp, x, v, w.zii, w.aii, device=dist.local) as e:
+            s0 = e.accel(True)
+            e0 = s0.ev + e.ttot()
+            ser = e.run(steps, 100)
+            es = np.array([ser[k].ev + ser[k].ek for k in range(99, steps, 100)])
+        out[prec] = {"E0": e0, "max_abs_dE_over_E": float(np.max(np.abs(es - e0)) / abs(e0)),
+                     "end_dE_over_E": float((es[-1] - e0) / abs(e0))}
+    out["target"] = "max |dE/E| <= 1e-5"
+    out["wall_s"] = time.perf_counter() - t0
+    return out
+
+
+def served_ensemble(args, dist):
+    """The 256-replica ensemble (256 pure-ion boxes, N log-uniform in
+    [1e3, 2e4], Gamma U[50, 250], kappa U[0.5, 2], Z in {6, 8, 26}, 1,000 steps
+    each, mixed precision) served with Poisson arrivals: p50 / p99 completion
+    latency and aggregate pair-interactions/s."""
+    from yukawamd_b200 import abi, configs
+    from yukawamd_b200.serve import Request, Server
+    seed = args.seed + 2 + 1000 * dist.rank
+    boxes = configs.replica_ensemble(seed)
+    rng = np.random.default_rng(np.random.PCG64(seed + 77))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.served_rate, len(boxes)))
+    arrivals -= arrivals[0]
+    reqs = [Request(i, w, args.ensemble_serve_steps, abi.YK_PREC_MIXED, float(t))
+            for i, (w, t) in enumerate(zip(boxes, arrivals))]
+    rep = Server(device=dist.local, chunk=50).run(reqs)
+    rep.pop("fp64_shadows", None)
+    rep["stream"] = ("256 pure-ion boxes, N log-uniform in [1e3, 2e4], Gamma U[50,250], kappa U[0.5,2], "
+                     "Z in {6,8,26}, seed %d, %d steps each, mixed precision, Poisson arrivals at %.0f runs/s "
+                     "(the last at %.2f s)" % (seed, args.ensemble_serve_steps, args.served_rate, arrivals[-1]))
+    return rep
 
 
 def nucleon_pair(K, W, me, dist):
@@ -523,37 +612,9 @@ def ensemble(steps, me, dist, precision="mixed", seed=4):
 
 
 def drift(args, dist):
-    """Total energy E = ev + ek (per particle) every 100 steps over args.drift
-    steps, FP64 and mixed, from the same equilibrated state; reports max |dE/E|.
-    The state comes from the reference's warm-up (md.F:87-101): args.drift_warmup
-    groups of 100 FP64 steps, each followed by cancel_vcom and tnorm, all on the
-    device through the run driver."""
-    from yukawamd_b200 import abi
-    from yukawamd_b200.driver import RunControl, run_md
-    from yukawamd_b200.engine import Engine
+    """--drift N: the drift block alone, for N steps of the chosen workload."""
     w = make_workload(args.workload, args.seed, args.n)
-    out = {"workload": workload_desc(w, args.workload), "steps": args.drift, "every": 100,
-           "warmup": "%d groups x 100 FP64 steps with cancel_vcom + tnorm (md.F:87-101)" % args.drift_warmup}
-    x, v = w.x, w.v
-    if args.drift_warmup > 0:
-        with Engine(w, device=dist.local, precision=abi.YK_PREC_FP64) as e:
-            t0 = time.perf_counter()
-            res = run_md(e, RunControl(nwgroup=args.drift_warmup, nwsteps=100))
-            out["warmup_wall_s"] = time.perf_counter() - t0
-            out["E_initial_raw"] = res.initial["e"]
-            x, v, _vold, _a = e.get_state()
-    for prec in ("fp64", "mixed"):
-        yp = w.yk_params(precision=abi.YK_PREC_MIXED if prec == "mixed" else abi.YK_PREC_FP64)
-        with Engine(yp, x, v, w.zii, w.aii, device=dist.local) as e:
-            s0 = e.accel(True)
-            e0 = s0.ev + e.ttot()
-            t0 = time.perf_counter()
-            ser = e.run(args.drift, 100)
-            wall = time.perf_counter() - t0
-            es = np.array([ser[k].ev + ser[k].ek for k in range(99, args.drift, 100)])
-        out[prec] = {"E0": e0, "E_end": float(es[-1]), "max_abs_dE_over_E": float(np.max(np.abs(es - e0)) / abs(e0)),
-                     "end_dE_over_E": float((es[-1] - e0) / abs(e0)), "wall_s": wall}
-    return out
+    return drift_block(w, args.workload, args.drift, args.drift_warmup, dist)
 
 
 def serve_stream(args, dist):

@@ -258,6 +258,41 @@ YK_API int yk_batch_set_state(yk_batch* b, int rep, const double* x,
                               const double* a);
 
 /*
+ * Slots, for serving (no counterpart in the reference, which runs one box
+ * per process).  yk_batch_create_slots makes an empty batch of nslots slots
+ * that holds at most max_particles particles and max_pair_units half-pair
+ * units (T (T + 1) / 2 per box of T = ceil(n / 128) tiles) at once; proto
+ * gives the kind (ion or nucleon) and precision of every box it will hold.
+ * The boxes of yk_batch_create are slots 0 .. nrep-1 of a batch that is full.
+ *
+ * yk_batch_admit puts one box into a free slot (*slot) with a budget of
+ * `steps` newton steps, copies its x, v (NULL: zero), zii, aii in, orders it
+ * and makes its initial measuring force call (md.F:69) -- over its own work
+ * items only; the other boxes are neither moved nor recomputed.  out (may be
+ * NULL) receives its scalars.  YK_ERR_NOMEM when no slot, particle range,
+ * tile range or scratch is free (nothing changes then).
+ *
+ * yk_batch_run advances every held box by up to nsteps steps: a box whose
+ * budget runs out stops at exactly its budget (its later series entries are
+ * zero), also inside a CUDA graph.  series is nsteps * nslots long.
+ *
+ * yk_batch_steps_left: the remaining budget of every slot (left[nslots]; -1
+ * for an empty slot).  yk_batch_retire copies the box's state out (any
+ * pointer may be NULL) and frees its slot.  Call these between runs only.
+ */
+YK_API int yk_batch_create_slots(const yk_params* proto, int nslots,
+                                 long long max_particles,
+                                 long long max_pair_units, int device,
+                                 yk_batch** out);
+YK_API int yk_batch_admit(yk_batch* b, const yk_params* p, int n,
+                          const double* x, const double* v,
+                          const double* zii, const double* aii,
+                          long long steps, int* slot, yk_scalars* out);
+YK_API int yk_batch_retire(yk_batch* b, int slot, double* x, double* v,
+                           double* vold, double* a);
+YK_API int yk_batch_steps_left(yk_batch* b, int* left);
+
+/*
  * Engine tunables (not reference parameters): which force kernel runs and
  * how its work is cut.  yk_create picks defaults; the autotuner
  * (yukawamd_b200/tune.py) measures the alternatives and sets them here.

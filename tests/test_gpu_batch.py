@@ -54,6 +54,32 @@ def test_batch_accel_matches_single_boxes(gpu, kind, prec, tol):
             assert abs(sc[r].px - s.px) <= tol * abs(s.px)
 
 
+@pytest.mark.parametrize("prec,tol", [(abi.YK_PREC_FP64, 1e-12), (abi.YK_PREC_MIXED, 1e-6)],
+                         ids=["fp64", "mixed"])
+@pytest.mark.parametrize("kind", ["ion", "nucleon"])
+def test_batch_accel_matches_oracle(gpu, kind, prec, tol):
+    """Every box of a batch against the CPU oracle's accel
+    (int_ion_pure.f:98-254, int_ion_mix.f:105-295, int_nn.f:130-345) on the
+    same positions: forces and the packed sums by 2-norm, ev and px."""
+    from oracle.oracle import Oracle
+    orc = Oracle("double", threads=8)
+    boxes = ion_boxes() if kind == "ion" else nucleon_boxes()
+    with Batch(boxes, precision=prec, mix_mode=abi.YK_MIX_FIXED) as b:
+        sc = b.accel(True)
+        states = [b.get_state(r) for r in range(b.nrep)]
+    for r, w in enumerate(boxes):
+        n = w.n
+        if n < 2:
+            continue
+        p = w.yk_params(mix_mode=abi.YK_MIX_FIXED)
+        a_ref, s_ref = orc.accel(p, w.x, w.zii, w.aii, True)
+        ab = states[r][3]
+        assert _rel(ab[:3 * n], a_ref[:3 * n]) <= tol, (kind, r)
+        assert _rel(ab[3 * n:], a_ref[3 * n:]) <= max(tol, 1e-12) * 10, (kind, r)
+        assert abs(sc[r].ev - s_ref.ev) <= tol * abs(s_ref.ev), (kind, r)
+        assert abs(sc[r].px - s_ref.px) <= tol * abs(s_ref.px), (kind, r)
+
+
 def test_batch_steps_match_single_boxes(gpu):
     boxes = ion_boxes()[:4]
     steps, me = 60, 10

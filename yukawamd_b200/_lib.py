@@ -49,6 +49,10 @@ SIGNATURES = {
     "yk_batch_run": (C.c_int, [_ctx, C.c_int, C.c_int, _S, C.POINTER(C.c_double)]),
     "yk_batch_get_state": (C.c_int, [_ctx, C.c_int, _dp, _dp, _dp, _dp]),
     "yk_batch_set_state": (C.c_int, [_ctx, C.c_int, _dp, _dp, _dp, _dp]),
+    "yk_batch_create_slots": (C.c_int, [_P, C.c_int, C.c_longlong, C.c_longlong, C.c_int, C.POINTER(_ctx)]),
+    "yk_batch_admit": (C.c_int, [_ctx, _P, C.c_int, _dp, _dp, _dp, _dp, C.c_longlong, C.POINTER(C.c_int), _S]),
+    "yk_batch_retire": (C.c_int, [_ctx, C.c_int, _dp, _dp, _dp, _dp]),
+    "yk_batch_steps_left": (C.c_int, [_ctx, C.POINTER(C.c_int)]),
     "yk_get_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_set_tuning": (C.c_int, [_ctx, C.POINTER(abi.YkTuning)]),
     "yk_perf_enable": (C.c_int, [_ctx, C.c_int, C.c_size_t]),

@@ -280,6 +280,16 @@ static void setup_args(yk_ctx* c)
         // coordinate and box length is below SHADOW_EXACT; a margin of 2 leaves
         // room for coordinates up to 2 L.
         f.lo = (f.img_k && 2.0 * Lmax < SHADOW_EXACT) ? 1 : 0;
+        f.hilo = (2.0 * Lmax < SHADOW_EXACT) ? 1 : 0;
+        for (int k = 0; k < 3; ++k) {
+            // the hi-part displacement is exact and within 2^-8 fm of the
+            // reference's FP64 one, so |d| < L/2 - 2^-7 leaves the image
+            // decision unambiguous
+            const double t = 0.5 * p.xl[k] - std::ldexp(1.0, -7);
+            float tf = (float)t;
+            if ((double)tf > t) tf = std::nextafter(tf, 0.0f);
+            f.hLm[k] = t > 0.0 ? tf : 0.0f;
+        }
     }
     f.n = c->n;
     f.nuclear_on = p.nuclear_on;
@@ -491,12 +501,13 @@ static int enqueue_order(yk_ctx* c, bool sort)
     return k + 1;
 }
 
-// The mixed ion kernels have a variant that always takes the hi/lo shadow
-// displacement (k_force_pairs<..., true>), for boxes that allow it.
+// The mixed kernels have a variant that always takes the hi/lo shadow
+// displacement (k_force_pairs<..., true>), for boxes that allow it: fa.lo
+// for ions, fa.hilo for nucleons.
 template <int SIM, int PREC>
 static bool lo_path(const ForceArgs& fa)
 {
-    return PREC == PREC_MIXED && SIM != SIM_NUCLEON && fa.lo != 0;
+    return PREC == PREC_MIXED && (SIM == SIM_NUCLEON ? fa.hilo != 0 : fa.lo != 0);
 }
 
 // Persistent grid of a PB-thread kernel on device dev (the current device):
@@ -534,7 +545,7 @@ static int launch_force_t(yk_ctx* c)
         k_force_near<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
             c->pos, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
     } else if (lo_path<SIM, PREC>(c->fa)) {
-        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON) {
+        if constexpr (PREC == PREC_MIXED) {
             const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(c->dev);
             k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
                 c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
@@ -1597,7 +1608,7 @@ static void noalloc_force(int dev, cudaStream_t st, const double4* pos, const fl
                           const int* perm, const double* zii, const double* aii, double* a)
 {
     if (lo_path<SIM, PREC>(fa)) {
-        if constexpr (PREC == PREC_MIXED && SIM != SIM_NUCLEON) {
+        if constexpr (PREC == PREC_MIXED) {
             const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(dev);
             k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter,
                                                                                    fa, Si, Sj, Sm, err);

@@ -68,6 +68,13 @@ struct ForceArgs {
     // (screen_d_x2); Lh = box on the SHADOW_Q grid, Ll = box - Lh
     float Lh[3], Ll[3];
     int lo;                          // img_k and every box length below SHADOW_EXACT / 2
+    // mixed form, nucleons: hi/lo displacement with the screen's image
+    // integers (every box length below SHADOW_EXACT / 2); a pair whose hi-part
+    // displacement after the image shift is hLm or more from 0 on some axis
+    // (hLm = L/2 - 2^-7 fm, rounded down) takes the reference's exact FP64
+    // minimum image instead (pair_group_nn_lo)
+    int hilo;
+    float hLm[3];
 };
 
 // FP32 shadow positions ("posf") are stored tile by tile: tile t (slots
@@ -234,6 +241,57 @@ __device__ __forceinline__ float2 screen_d_x2(const ForceArgs& fa, const ScreenI
         float2 e = __fadd2_rn(lj, make_float2(nli[c], nli[c]));
         e = __ffma2_rn(make_float2(-fa.Ll[c], -fa.Ll[c]), k, e);
         d[c] = __fadd2_rn(d1, e);
+    }
+    float2 r2 = __fmul2_rn(d[2], d[2]);
+    r2 = __ffma2_rn(d[1], d[1], r2);
+    return __ffma2_rn(d[0], d[0], r2);
+}
+
+// screen_d_x2 for nucleons, also flagging (bits 0, 1 of flag for the two
+// pairs) the pairs whose hi-part displacement after the image shift is hLm
+// or more from 0 on some axis: the image decision of those pairs is close to
+// the reference's boundary |d| = L/2, and they take the exact FP64 image.
+__device__ __forceinline__ float2 screen_d_flag_x2(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
+                                                   const float* __restrict__ t, const float* __restrict__ tl,
+                                                   int g, int off, float2 (&d)[3], unsigned& flag)
+{
+    const float2 MAG = make_float2(12582912.0f, 12582912.0f);
+    const float2 NMAG = make_float2(-12582912.0f, -12582912.0f);
+    const float ni[3] = {si.nx, si.ny, si.nz};
+    unsigned f = 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float2 xj = *reinterpret_cast<const float2*>(t + c * 2 * SHADOW_TILE + 8 * g + off);
+        const float2 lj = *reinterpret_cast<const float2*>(tl + c * 2 * SHADOW_TILE + 8 * g + off);
+        const float2 dc = __fadd2_rn(xj, make_float2(ni[c], ni[c]));
+        const float2 k = __fadd2_rn(__ffma2_rn(dc, make_float2(fa.invLf[c], fa.invLf[c]), MAG), NMAG);
+        const float2 d1 = __ffma2_rn(make_float2(-fa.Lh[c], -fa.Lh[c]), k, dc);       // exact
+        f |= (fabsf(d1.x) >= fa.hLm[c] ? 1u : 0u) | (fabsf(d1.y) >= fa.hLm[c] ? 2u : 0u);
+        float2 e = __fadd2_rn(lj, make_float2(nli[c], nli[c]));
+        e = __ffma2_rn(make_float2(-fa.Ll[c], -fa.Ll[c]), k, e);
+        d[c] = __fadd2_rn(d1, e);
+    }
+    flag = f;
+    float2 r2 = __fmul2_rn(d[2], d[2]);
+    r2 = __ffma2_rn(d[1], d[1], r2);
+    return __ffma2_rn(d[0], d[0], r2);
+}
+
+// screen_d_x2 when the image of every reachable source of the tile is the
+// same, k per axis, and has been folded into the target's coordinates once
+// per tile: th = -(x_i hi part) - k Lh (exact on the SHADOW_Q grid), tl2 =
+// -(x_i lo part) - k Ll.  Per axis the exact hi-part difference plus the lo
+// correction, one rounding: d = x_j - x_i - k L to FP32 precision.  Returns
+// r^2.
+__device__ __forceinline__ float2 disp_tile_x2(const float2 (&th)[3], const float2 (&tl2)[3],
+                                               const float* __restrict__ t, const float* __restrict__ tl, int g,
+                                               int off, float2 (&d)[3])
+{
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float2 xj = *reinterpret_cast<const float2*>(t + c * 2 * SHADOW_TILE + 8 * g + off);
+        const float2 lj = *reinterpret_cast<const float2*>(tl + c * 2 * SHADOW_TILE + 8 * g + off);
+        d[c] = __fadd2_rn(__fadd2_rn(xj, th[c]), __fadd2_rn(lj, tl2[c]));
     }
     float2 r2 = __fmul2_rn(d[2], d[2]);
     r2 = __ffma2_rn(d[1], d[1], r2);
@@ -496,6 +554,45 @@ __device__ __forceinline__ void ion_terms_x2(const ForceArgs& fa, float2 r2, flo
     if constexpr (MEAS) {
         u = __fmul2_rn(__fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf)), msk);
         w = __fmul2_rn(fs, r2);
+    }
+}
+
+// The nucleon terms for two pairs in the mixed form (int_nn.f:208-229), the
+// FP32 arithmetic paired; r2 their r^2, msk 1 for a pair that takes the term
+// and 0 otherwise.  Adds to fs (and u, w when measuring).
+//   nuclear: e = exp(-r^2 / (2 Lambda)), B = bb + cc (like pair) or bb - cc,
+//            fn = (2 aa e + B) e / Lambda, u = (aa e + B) e, w = fn r^2
+//   p-p Coulomb: fc = vc (1 + mu r) e^{-mu r} / r^3, u = vc e^{-mu r}/r - evcut
+//            (evcut includes vc for nucleons), w = fc r^2
+template <bool MEAS>
+__device__ __forceinline__ void nuclear_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2 B, float2& fs,
+                                                 float2& u, float2& w)
+{
+    const float2 e = exp_neg_f32_xu_x2(__fmul2_rn(r2, make_float2(fa.xp2if, fa.xp2if)));
+    const float2 em = __fmul2_rn(e, msk);
+    const float2 fn = __fmul2_rn(make_float2(fa.xpif, fa.xpif),
+                                 __fmul2_rn(__ffma2_rn(make_float2(fa.aa2f, fa.aa2f), e, B), em));
+    fs = __fadd2_rn(fs, fn);
+    if constexpr (MEAS) {
+        u = __ffma2_rn(__ffma2_rn(make_float2(fa.aaf, fa.aaf), e, B), em, u);
+        w = __ffma2_rn(fn, r2, w);
+    }
+}
+
+template <bool MEAS>
+__device__ __forceinline__ void coulomb_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2& fs, float2& u,
+                                                 float2& w)
+{
+    const float2 r2s = make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f);
+    const float2 rinv = make_float2(rsqrt_f32(r2s.x), rsqrt_f32(r2s.y));
+    const float2 mr = __fmul2_rn(make_float2(fa.xmucf, fa.xmucf), __fmul2_rn(r2s, rinv));
+    const float2 er = __fmul2_rn(__fmul2_rn(exp_neg_f32_xu_x2(mr), rinv), make_float2(fa.vcf, fa.vcf));
+    const float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(make_float2(1.0f, 1.0f), mr), er), __fmul2_rn(rinv, rinv));
+    const float2 fc = __fmul2_rn(f, msk);
+    fs = __fadd2_rn(fs, fc);
+    if constexpr (MEAS) {
+        u = __ffma2_rn(__fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf)), msk, u);
+        w = __ffma2_rn(fc, r2, w);
     }
 }
 

@@ -229,17 +229,25 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
 // displacement (fa.lo): the screen computes the final displacement and r^2
 // (screen_d_x2), so its mask is the cutoff test itself and the pair terms
 // need no FP64 source tile.  tll is the tile's lo part, nli the target's
-// negated lo parts.
-template <int SIM, bool MEAS, bool CHECK>
+// negated lo parts.  TILEIMG: the tile's reachable sources share one image,
+// folded into th / tl2 (disp_tile_x2), so no pair takes its own image.
+template <int SIM, bool MEAS, bool CHECK, bool TILEIMG = false>
 __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
+                                              const float2 (&th)[3], const float2 (&tl2)[3],
                                               float wi, const float* tlf, const float* tll, int j0, int jlim,
                                               bool diag, bool active, int tid, int sw,
                                               TargetAcc<PREC_MIXED, MEAS>& acc, float* my_acc)
 {
     const int g = j0 >> 2;
     float2 da[3], db[3];
-    const float2 ra = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * sw, da);
-    const float2 rb = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * (sw ^ 2), db);
+    float2 ra, rb;
+    if constexpr (TILEIMG) {
+        ra = disp_tile_x2(th, tl2, tlf, tll, g, 2 * sw, da);
+        rb = disp_tile_x2(th, tl2, tlf, tll, g, 2 * (sw ^ 2), db);
+    } else {
+        ra = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * sw, da);
+        rb = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * (sw ^ 2), db);
+    }
     unsigned m = (ra.x <= fa.rc2f ? 1u : 0u) | (ra.y <= fa.rc2f ? 2u : 0u) | (rb.x <= fa.rc2f ? 4u : 0u) |
                  (rb.y <= fa.rc2f ? 8u : 0u);
     if constexpr (CHECK) {
@@ -309,6 +317,121 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
     }
 }
 
+// pair_group for nucleons in the mixed form (fa.hilo): the hi/lo FP32
+// displacement with the screen's image integers (screen_d_flag_x2); the
+// pairs that the screen flags as close to |d| = L/2 on some axis take the
+// reference's conditional minimum image on the FP64 positions instead
+// (int_nn.f:190-195; gsrc is the tile's FP64 slots in global memory), so every
+// pair gets the reference's image.  Then the HPP terms inside rncut and the
+// p-p Coulomb inside rccut (int_nn.f:208-229), two pairs per FP32x2
+// instruction, a branch per term only when no lane of the warp needs it.
+template <bool MEAS, bool CHECK>
+__device__ __forceinline__ void pair_group_nn_lo(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
+                                                 const double4& pi, const float* tlf, const float* tll,
+                                                 const double4* __restrict__ gsrc, int j0, int jlim, bool diag,
+                                                 bool active, int tid, int sw, TargetAcc<PREC_MIXED, MEAS>& acc,
+                                                 float* my_acc)
+{
+    const int g = j0 >> 2;
+    float2 da[3], db[3];
+    unsigned fla = 0, flb = 0;
+    float2 ra = screen_d_flag_x2(fa, si, nli, tlf, tll, g, 2 * sw, da, fla);
+    float2 rb = screen_d_flag_x2(fa, si, nli, tlf, tll, g, 2 * (sw ^ 2), db, flb);
+    unsigned ok = 0xfu;
+    if constexpr (CHECK) {
+        ok = 0;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const int jl = j0 + (jj ^ sw);
+            if (active && jl < jlim && (!diag || jl > tid)) ok |= 1u << jj;
+        }
+    }
+    const unsigned fl = (fla | (flb << 2)) & ok;
+    if (__any_sync(0xffffffffu, fl != 0)) {
+        // d = x_j - x_i from the reference's d = x_i - x_j and its image
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            if ((fl >> jj) & 1u) {
+                const double4 pj = gsrc[j0 + (jj ^ sw)];
+                const float ex = -__double2float_rn(min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]));
+                const float ey = -__double2float_rn(min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]));
+                const float ez = -__double2float_rn(min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]));
+                const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                float2(&dd)[3] = jj < 2 ? da : db;
+                float2& rr = jj < 2 ? ra : rb;
+                if (jj & 1) {
+                    dd[0].y = ex;
+                    dd[1].y = ey;
+                    dd[2].y = ez;
+                    rr.y = r2;
+                } else {
+                    dd[0].x = ex;
+                    dd[1].x = ey;
+                    dd[2].x = ez;
+                    rr.x = r2;
+                }
+            }
+        }
+    }
+    const float* tw = tlf + 6 * SHADOW_TILE + j0;
+    const float wj[4] = {tw[sw], tw[sw ^ 1], tw[sw ^ 2], tw[sw ^ 3]};
+    const float r2v[4] = {ra.x, ra.y, rb.x, rb.y};
+    const bool ip = si.w == 1.0f;
+    unsigned mn = 0, mc = 0;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+        const bool in = (ok >> jj) & 1u;
+        if (in && fa.nuclear_on && r2v[jj] <= fa.rn2f) mn |= 1u << jj;
+        if (in && fa.coulomb_on && ip && wj[jj] == 1.0f && r2v[jj] <= fa.rc2f) mc |= 1u << jj;
+    }
+    const bool any_n = __any_sync(0xffffffffu, mn != 0);
+    const bool any_c = __any_sync(0xffffffffu, mc != 0);
+    if (!any_n && !any_c) return;
+    float2 fsa = make_float2(0.f, 0.f), fsb = fsa, ua = fsa, ub = fsa, wa = fsa, wb = fsa;
+    if (any_n) {
+        const float2 Ba = make_float2(wj[0] == si.w ? fa.bpcf : fa.bmcf, wj[1] == si.w ? fa.bpcf : fa.bmcf);
+        const float2 Bb = make_float2(wj[2] == si.w ? fa.bpcf : fa.bmcf, wj[3] == si.w ? fa.bpcf : fa.bmcf);
+        nuclear_terms_x2<MEAS>(fa, ra, make_float2((mn & 1u) ? 1.f : 0.f, (mn & 2u) ? 1.f : 0.f), Ba, fsa, ua, wa);
+        nuclear_terms_x2<MEAS>(fa, rb, make_float2((mn & 4u) ? 1.f : 0.f, (mn & 8u) ? 1.f : 0.f), Bb, fsb, ub, wb);
+    }
+    if (any_c) {
+        coulomb_terms_x2<MEAS>(fa, ra, make_float2((mc & 1u) ? 1.f : 0.f, (mc & 2u) ? 1.f : 0.f), fsa, ua, wa);
+        coulomb_terms_x2<MEAS>(fa, rb, make_float2((mc & 4u) ? 1.f : 0.f, (mc & 8u) ? 1.f : 0.f), fsb, ub, wb);
+    }
+    // F_i += fs (x_i - x_j) = -fs d (int_nn.f:230-240); the reaction on j is fs d
+    GroupSum<PREC_MIXED, MEAS> gs;
+    float2 fxa[3], fxb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        fxa[c] = __fmul2_rn(fsa, da[c]);
+        fxb[c] = __fmul2_rn(fsb, db[c]);
+        const float2 sc = __fadd2_rn(fxa[c], fxb[c]);
+        gs.f[c] = -(sc.x + sc.y);
+    }
+    if constexpr (MEAS) {
+        const float2 su = __fadd2_rn(ua, ub);
+        const float2 sv = __fadd2_rn(wa, wb);
+        gs.s[0] = su.x + su.y;
+        gs.s[1] = sv.x + sv.y;
+        const int P[6] = {0, 0, 0, 1, 1, 2}, Q[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float2 sp = __ffma2_rn(db[P[k]], fxb[Q[k]], __fmul2_rn(da[P[k]], fxa[Q[k]]));
+            gs.s[2 + k] = sp.x + sp.y;
+        }
+    }
+    acc.add_group2(gs);
+    float t[3];
+    reduce_scatter4_x2(fxa, fxb, t);
+    const int lane = threadIdx.x & 31;
+    const int jl = j0 + sw;
+    if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
+        my_acc[3 * jl] = t[0];
+        my_acc[3 * jl + 1] = t[1];
+        my_acc[3 * jl + 2] = t[2];
+    }
+}
+
 // ---- which source groups can reach a warp's targets ----------------------
 // The bounding box of a warp's active targets (FP32 copies), computed once per
 // job; a source farther than the screening radius from the box (in the
@@ -321,6 +444,10 @@ struct WarpBox {
     float lo[3], hi[3];
     float c[3], h[3];                // centre and half-width plus the rounding margin
     bool any, has_p;                 // any active target; any proton target (nucleons)
+    // 2 (r_c + h) < L - 2 fm on every axis: then the one image of a tile's
+    // reachable sources seen from the centre is the minimum image of every
+    // pair inside r_c (near_groups_img)
+    bool tile_img;
 };
 
 __device__ __forceinline__ float warp_minf(float v)
@@ -356,6 +483,20 @@ __device__ __forceinline__ WarpBox warp_box(const ForceArgs& fa, const double4& 
     }
     b.any = __any_sync(0xffffffffu, active);
     b.has_p = __any_sync(0xffffffffu, active && pi.w == 1.0);
+    // A pair inside r_c has |d| <= r_c < L/2 per axis in its minimum image.
+    // Seen from the centre, a reachable source lies within r_c + h per axis
+    // of the image k that the centre gives it, and a target within h, so the
+    // pair's displacement with image k is within r_c + 2h < L - r_c per axis:
+    // any other image would put the pair farther than L - r_c > r_c, so k is
+    // the pair's minimum image.  Pairs outside r_c stay outside under any
+    // image.  (scr_c2 is the widened screening radius; 1 fm of slack.)
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float t = 0.5f * fa.Lf[k] - b.h[k] - 1.0f;
+        ok = ok && t > 0.f && t * t > fa.scr_c2;
+    }
+    b.tile_img = ok;
     return b;
 }
 
@@ -395,6 +536,64 @@ __device__ __forceinline__ unsigned any_of_4(unsigned v)
     v = (v | (v >> 6)) & 0x000f000fu;
     v = (v | (v >> 12)) & 0xffu;
     return v;
+}
+
+// box_reaches, also returning the image the centre gives the source: per axis
+// k = rint((x - c) / L) in {-1, 0, 1}, as the low 2 bits (two's complement)
+// of the magic-number sum, packed 2 bits per axis.
+__device__ __forceinline__ bool box_reaches_img(const ForceArgs& fa, const WarpBox& b, const float (&x)[3],
+                                                unsigned& code)
+{
+    const float MAGIC = 12582912.0f;
+    float dist2 = 0.f;
+    unsigned cd = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float d = x[k] - b.c[k];
+        const float kb = fmaf(d, fa.invLf[k], MAGIC);
+        const float dm = fmaf(-fa.Lf[k], kb - MAGIC, d);
+        const float m = fmaxf(fabsf(dm) - b.h[k], 0.f);
+        dist2 = fmaf(m, m, dist2);
+        cd |= (__float_as_uint(kb) & 3u) << (2 * k);
+    }
+    code = cd;
+    return dist2 <= fa.scr_c2;
+}
+
+// Image of axis c from a packed code: 0 -> 0, 1 -> +1, 3 -> -1.
+__device__ __forceinline__ float img_of(int code, int c)
+{
+    const int b = (code >> (2 * c)) & 3;
+    return b == 0 ? 0.f : (b == 1 ? 1.f : -1.f);
+}
+
+// near_groups for ions, also telling whether all reachable sources of the
+// tile take the same image from the warp's centre: kcode = their packed
+// image code, or -1 if they differ (or none is reachable).
+__device__ __forceinline__ unsigned near_groups_img(const ForceArgs& fa, const WarpBox& b,
+                                                    const float* __restrict__ tlf, int jlim, int jmin, int& kcode)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned gm = 0, c_and = 0x3fu, c_or = 0u;
+#pragma unroll
+    for (int blk = 0; blk < PB / 32; ++blk) {
+        const int j = 32 * blk + lane;
+        bool near = false;
+        unsigned code = 0;
+        if (b.any && j < jlim && j >= jmin) {
+            const float x[3] = {tlf[shadow_off(j, 0)], tlf[shadow_off(j, 1)], tlf[shadow_off(j, 2)]};
+            near = box_reaches_img(fa, b, x, code);
+        }
+        if (near) {
+            c_and &= code;
+            c_or |= code;
+        }
+        gm |= any_of_4(__ballot_sync(0xffffffffu, near)) << (8 * blk);
+    }
+    c_and = __reduce_and_sync(0xffffffffu, c_and);
+    c_or = __reduce_or_sync(0xffffffffu, c_or);
+    kcode = (gm != 0 && c_and == c_or) ? (int)c_or : -1;
+    return gm;
 }
 
 template <int SIM>
@@ -515,10 +714,12 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
     const WarpBox box = warp_box(fa, pi, active);
     TargetAcc<PREC, MEAS> acc;
     acc.zero();
-    // mixed-form ions on a box that allows it: FP32 displacements from the
-    // shadow's hi/lo parts, no FP64 source tiles
-    const bool lo = (PREC == PREC_MIXED) && (SIM == SIM_PURE || SIM == SIM_MIX) &&
-                    (LOMODE == 1 || (LOMODE == 2 && fa.lo != 0));
+    // the mixed form on a box that allows it: FP32 displacements from the
+    // shadow's hi/lo parts, no FP64 source tiles (ions: fa.lo; nucleons:
+    // fa.hilo, with the FP64 positions read from global memory for the rare
+    // pairs near |d| = L/2)
+    const bool lo = (PREC == PREC_MIXED) &&
+                    (LOMODE == 1 || (LOMODE == 2 && (SIM == SIM_NUCLEON ? fa.hilo != 0 : fa.lo != 0)));
     float nli[3] = {0.f, 0.f, 0.f};
     if (lo) {
 #pragma unroll
@@ -544,28 +745,74 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
         for (int k = lane; k < PB * 3; k += 32) my_acc[k] = 0.0;
         __syncwarp();
         // on the diagonal tile only sources after the warp's first target count
-        unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, diag ? 32 * warp + 1 : 0);
+        const int jmin = diag ? 32 * warp + 1 : 0;
         if (lo) {
-            if constexpr (PREC == PREC_MIXED && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+            if constexpr (PREC == PREC_MIXED && SIM == SIM_NUCLEON) {
+                unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
                 const float* tll = reinterpret_cast<const float*>(tl);
+                const double4* gsrc = bx.pos + (size_t)C * PB;
                 if (!diag && jlim == PB && all_active) {
                     for (; gm; gm &= gm - 1)
-                        pair_group_lo<SIM, MEAS, false>(fa, si, nli, wi, tlf, tll, 4 * (__ffs(gm) - 1), jlim,
-                                                        diag, active, tid, sw, acc, my_acc);
+                        pair_group_nn_lo<MEAS, false>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
+                                                      diag, active, tid, sw, acc, my_acc);
                 } else {
                     for (; gm; gm &= gm - 1)
-                        pair_group_lo<SIM, MEAS, true>(fa, si, nli, wi, tlf, tll, 4 * (__ffs(gm) - 1), jlim,
-                                                       diag, active, tid, sw, acc, my_acc);
+                        pair_group_nn_lo<MEAS, true>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
+                                                     diag, active, tid, sw, acc, my_acc);
                 }
             }
-        } else if (!diag && jlim == PB && all_active) {
-            for (; gm; gm &= gm - 1)
-                pair_group<SIM, PREC, MEAS, false, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
-                                                   active, tid, sw, acc, my_acc);
+            if constexpr (PREC == PREC_MIXED && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+                int kcode = -1;
+                unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
+                const float* tll = reinterpret_cast<const float*>(tl);
+                const bool full = !diag && jlim == PB && all_active;
+                if (box.tile_img && kcode >= 0) {
+                    // one image for the whole tile: fold it into the target
+                    float2 th[3], tl2[3];
+                    const float nh[3] = {si.nx, si.ny, si.nz};
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float k = img_of(kcode, c);
+                        const float h = fmaf(-k, fa.Lh[c], nh[c]);       // exact
+                        const float l = fmaf(-k, fa.Ll[c], nli[c]);
+                        th[c] = make_float2(h, h);
+                        tl2[c] = make_float2(l, l);
+                    }
+                    if (full) {
+                        for (; gm; gm &= gm - 1)
+                            pair_group_lo<SIM, MEAS, false, true>(fa, si, nli, th, tl2, wi, tlf, tll,
+                                                                  4 * (__ffs(gm) - 1), jlim, diag, active, tid,
+                                                                  sw, acc, my_acc);
+                    } else {
+                        for (; gm; gm &= gm - 1)
+                            pair_group_lo<SIM, MEAS, true, true>(fa, si, nli, th, tl2, wi, tlf, tll,
+                                                                 4 * (__ffs(gm) - 1), jlim, diag, active, tid,
+                                                                 sw, acc, my_acc);
+                    }
+                } else {
+                    const float2 z[3] = {};
+                    if (full) {
+                        for (; gm; gm &= gm - 1)
+                            pair_group_lo<SIM, MEAS, false>(fa, si, nli, z, z, wi, tlf, tll, 4 * (__ffs(gm) - 1),
+                                                            jlim, diag, active, tid, sw, acc, my_acc);
+                    } else {
+                        for (; gm; gm &= gm - 1)
+                            pair_group_lo<SIM, MEAS, true>(fa, si, nli, z, z, wi, tlf, tll, 4 * (__ffs(gm) - 1),
+                                                           jlim, diag, active, tid, sw, acc, my_acc);
+                    }
+                }
+            }
         } else {
-            for (; gm; gm &= gm - 1)
-                pair_group<SIM, PREC, MEAS, true, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim, diag,
-                                                  active, tid, sw, acc, my_acc);
+            unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
+            if (!diag && jlim == PB && all_active) {
+                for (; gm; gm &= gm - 1)
+                    pair_group<SIM, PREC, MEAS, false, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                                                             diag, active, tid, sw, acc, my_acc);
+            } else {
+                for (; gm; gm &= gm - 1)
+                    pair_group<SIM, PREC, MEAS, true, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                                                            diag, active, tid, sw, acc, my_acc);
+            }
         }
         // this warp is done with the tile: the last warp reduces and refills
         __threadfence_block();

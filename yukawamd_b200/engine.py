@@ -304,6 +304,56 @@ class Batch:
             pass
 
 
+class SlotBatch(Batch):
+    """A batch of fixed capacity that runs enter and leave one at a time
+    (yk_batch_create_slots / yk_batch_admit / yk_batch_retire): the serving
+    loop's device-resident group.  proto: YkParams of the kind (ion or
+    nucleon) and precision of every box it will hold.  Slots are indexed
+    0 .. nslots-1; run()'s series is indexed [step * nslots + slot]."""
+
+    def __init__(self, proto, nslots, max_particles, max_pair_units, device=0):
+        self._lib = lib()
+        self._b = C.c_void_p()
+        self.nrep = int(nslots)
+        self.n = [0] * self.nrep
+        check_batch(self._lib.yk_batch_create_slots(C.byref(proto), self.nrep, int(max_particles),
+                                                    int(max_pair_units), int(device), C.byref(self._b)))
+
+    @staticmethod
+    def pair_units(n):
+        t = (int(n) + 127) // 128
+        return t * (t + 1) // 2
+
+    def admit(self, params, x, v, zii, aii, steps):
+        """Admit one box with a budget of `steps` steps; returns (slot, its
+        scalars after the initial measuring force call).  Raises EngineError
+        with code YK_ERR_NOMEM when it does not fit."""
+        x, v, zii, aii = _f64(x), _f64(v), _f64(zii), _f64(aii)
+        n = len(x) // 3
+        slot = C.c_int(-1)
+        out = abi.YkScalars()
+        check_batch(self._lib.yk_batch_admit(self._b, C.byref(params), n, _ptr(x), _ptr(v), _ptr(zii), _ptr(aii),
+                                             int(steps), C.byref(slot), C.byref(out)), self._b)
+        self.n[slot.value] = n
+        return slot.value, out
+
+    def retire(self, slot):
+        """The box's final (x, v, vold, a); its slot is free afterwards."""
+        n = self.n[slot]
+        x, v, vold = (np.empty(3 * n) for _ in range(3))
+        a = np.empty(3 * (n + 3))
+        check_batch(self._lib.yk_batch_retire(self._b, int(slot), _ptr(x), _ptr(v), _ptr(vold), _ptr(a)),
+                    self._b)
+        self.n[slot] = 0
+        return x, v, vold, a
+
+    def steps_left(self):
+        """Remaining step budget per slot (-1 for an empty slot)."""
+        out = (C.c_int * self.nrep)()
+        check_batch(self._lib.yk_batch_steps_left(self._b, out), self._b)
+        return np.array(out[:], dtype=np.int64)
+
+
 def kernel_launch_count():
     return int(lib().yk_kernel_launch_count())
 
