@@ -131,12 +131,11 @@ __global__ void k_b_repack(const int* __restrict__ iperm, const int* __restrict_
 }
 
 // vel_verlet_2.f:33-54 for every box (block table: box, block within box;
-// entries of box -1 are unused).
+// entries of box -1 are unused), in the caller's order: every read and
+// write is coalesced.  The slot-ordered copies follow in k_b_pack.
 __global__ void __launch_bounds__(VBLOCK)
 k_b_drift(const int2* __restrict__ vb, const RepDesc* __restrict__ rd, const int* __restrict__ left,
-          double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold, const double* __restrict__ a,
-          const double* __restrict__ zii, const int* __restrict__ iperm, double4* __restrict__ pos,
-          float* __restrict__ posf)
+          double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold, const double* __restrict__ a)
 {
     const int2 t = vb[blockIdx.x];
     if (t.x < 0 || left[t.x] <= 0) return;
@@ -146,17 +145,33 @@ k_b_drift(const int2* __restrict__ vb, const RepDesc* __restrict__ rd, const int
     if (local >= s.n) return;
     const int gi = d->P + local;
     const double* ar = a + d->A;
-    double xn[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const int e = 3 * gi + k;
         const double vi = v[e], ai = ar[3 * local + k];
-        xn[k] = drift1(x[e], vi, ai, s, k);
-        x[e] = xn[k];
+        x[e] = drift1(x[e], vi, ai, s, k);
         vold[e] = vi;
         v[e] = __dadd_rn(vi, __dmul_rn(s.dt, ai));
     }
-    store_pos(pos, posf, iperm[gi], xn, zii[gi]);
+}
+
+// The slot-ordered FP64 positions and FP32 shadow of every box that steps, a
+// thread per slot: the position is gathered through perm and the slot's
+// words are written in slot order (a warp writes contiguous runs), instead of
+// being scattered through the permutation by the drift kernel.
+__global__ void __launch_bounds__(256)
+k_b_pack(const int* __restrict__ tile_rep, const RepDesc* __restrict__ rd, const int* __restrict__ left,
+         const int* __restrict__ perm, const double* __restrict__ x, const double* __restrict__ zii,
+         double4* __restrict__ pos, float* __restrict__ posf, int total_slots)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= total_slots) return;
+    const int r = tile_rep[p >> 7];
+    if (r < 0 || left[r] <= 0) return;
+    if (p - rd[r].S >= rd[r].fa.n) return;
+    const int o = perm[p];
+    const double xn[3] = {x[3 * o], x[3 * o + 1], x[3 * o + 2]};
+    store_pos(pos, posf, p, xn, zii[o]);
 }
 
 // vel_verlet_2.f:75-95 for every box; kinetic partials per block.
@@ -504,9 +519,10 @@ static int enqueue_step_b(yk_batch* b, bool meas, bool series, bool resort)
         b->pos_dirty = false;
         ++k;
     }
-    k_b_drift<<<b->vb_cap, VBLOCK, 0, st>>>(b->vblocks, b->rd, b->left, b->x, b->v, b->vold, b->a, b->zii,
-                                           b->iperm, b->pos, b->posf);
-    ++k;
+    k_b_drift<<<b->vb_cap, VBLOCK, 0, st>>>(b->vblocks, b->rd, b->left, b->x, b->v, b->vold, b->a);
+    k_b_pack<<<(b->tcap * PB + 255) / 256, 256, 0, st>>>(b->tile_rep, b->rd, b->left, b->perm, b->x, b->zii,
+                                                          b->pos, b->posf, b->tcap * PB);
+    k += 2;
     k += enqueue_force_b(b, meas);
     if (meas)
         k_b_post<true><<<b->vb_cap, VBLOCK, 0, st>>>(b->vblocks, b->rd, b->left, b->v, b->vold, b->a, b->aii,

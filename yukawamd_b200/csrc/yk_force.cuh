@@ -473,6 +473,35 @@ __device__ __forceinline__ double image_k(const ForceArgs& fa, double d, float k
     return fa.img_k ? __fma_rn((double)k, fa.xl[c], d) : min_image(d, fa.xl[c], fa.hlb[c]);
 }
 
+// The FP32 screen's r^2 when the tile's image is folded into the target
+// (th as in disp_tile_x2; hi parts only, so the screening radius is the
+// widened one).
+__device__ __forceinline__ float2 screen_r2_tile_x2(const float2 (&th)[3], const float* __restrict__ t, int g,
+                                                    int off)
+{
+    float2 d[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        d[c] = __fadd2_rn(*reinterpret_cast<const float2*>(t + c * 2 * SHADOW_TILE + 8 * g + off), th[c]);
+    float2 r2 = __fmul2_rn(d[2], d[2]);
+    r2 = __ffma2_rn(d[1], d[1], r2);
+    return __ffma2_rn(d[0], d[0], r2);
+}
+
+template <int PREC, bool MEAS>
+__device__ __forceinline__ void ion_terms_nb(const ForceArgs& fa, double dx, double dy, double dz, bool sel,
+                                             PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o);
+
+// ion_pair_nb when the tile's image k is folded into the target: pit =
+// x_i + k L (per axis), so d = pit - x_j is the pair's minimum image for
+// every pair inside r_c.
+template <int PREC, bool MEAS>
+__device__ __forceinline__ void ion_pair_tile(const ForceArgs& fa, const double4& pit, const double4& pj, bool sel,
+                                              PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o)
+{
+    ion_terms_nb<PREC, MEAS>(fa, __dsub_rn(pit.x, pj.x), __dsub_rn(pit.y, pj.y), __dsub_rn(pit.z, pj.z), sel, o);
+}
+
 template <int PREC, bool MEAS, bool IMGK = false>
 __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& pi, const double4& pj, bool sel,
                                             const float (&k)[3],
@@ -481,6 +510,14 @@ __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& 
     const double dx = image_k<IMGK>(fa, __dsub_rn(pi.x, pj.x), k[0], 0);
     const double dy = image_k<IMGK>(fa, __dsub_rn(pi.y, pj.y), k[1], 1);
     const double dz = image_k<IMGK>(fa, __dsub_rn(pi.z, pj.z), k[2], 2);
+    ion_terms_nb<PREC, MEAS>(fa, dx, dy, dz, sel, o);
+}
+
+// The pair terms of ion_pair_nb from the minimum-image displacement.
+template <int PREC, bool MEAS>
+__device__ __forceinline__ void ion_terms_nb(const ForceArgs& fa, double dx, double dy, double dz, bool sel,
+                                             PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o)
+{
     if constexpr (PREC == PREC_FP64) {
         o.dx = dx;
         o.dy = dy;

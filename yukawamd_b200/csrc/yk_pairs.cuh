@@ -137,17 +137,27 @@ __device__ __forceinline__ void reduce_scatter4(T (&r)[4][3], T (&t)[3])
 // one at 2 (sw ^ 2)), so each step's image integers are plain registers.
 // CHECK: the tile is partial, diagonal, or the CTA has inactive targets, so
 // every pair needs the validity test.
-template <int SIM, int PREC, bool MEAS, bool CHECK, bool IMGK = false>
+// TILEIMG (ions): the tile's reachable sources share one image, folded into
+// th (the screen's target hi parts) and pit (the FP64 target position), so no
+// pair takes its own image.
+template <int SIM, int PREC, bool MEAS, bool CHECK, bool IMGK = false, bool TILEIMG = false>
 __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& pi, const ScreenI& si,
                                            real_t<PREC> wi, const double4* tl, const float* tlf,
                                            int j0, int jlim, bool diag, bool active, int tid,
-                                           int sw, TargetAcc<PREC, MEAS>& acc, row_t<PREC>* my_acc)
+                                           int sw, TargetAcc<PREC, MEAS>& acc, row_t<PREC>* my_acc,
+                                           const float2 (&th)[3] = {}, const double4& pit = double4{})
 {
     using R_t = real_t<PREC>;
     const int g = j0 >> 2;
     float2 ka[3], kb[3];
-    const float2 ra = screen_r2k_x2(fa, si, tlf, g, 2 * sw, ka);
-    const float2 rb = screen_r2k_x2(fa, si, tlf, g, 2 * (sw ^ 2), kb);
+    float2 ra, rb;
+    if constexpr (TILEIMG) {
+        ra = screen_r2_tile_x2(th, tlf, g, 2 * sw);
+        rb = screen_r2_tile_x2(th, tlf, g, 2 * (sw ^ 2));
+    } else {
+        ra = screen_r2k_x2(fa, si, tlf, g, 2 * sw, ka);
+        rb = screen_r2k_x2(fa, si, tlf, g, 2 * (sw ^ 2), kb);
+    }
     const float* tw = tlf + 6 * SHADOW_TILE + j0;
     unsigned m = (ra.x <= screen_lim<SIM>(fa, si.w, tw[sw]) ? 1u : 0u) |
                  (ra.y <= screen_lim<SIM>(fa, si.w, tw[sw ^ 1]) ? 2u : 0u) |
@@ -174,11 +184,15 @@ __device__ __forceinline__ void pair_group(const ForceArgs& fa, const double4& p
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
             const double4 pjv = tl[j0 + (jj ^ sw)];
-            const float k[3] = {jj == 0 ? ka[0].x : jj == 1 ? ka[0].y : jj == 2 ? kb[0].x : kb[0].y,
-                                jj == 0 ? ka[1].x : jj == 1 ? ka[1].y : jj == 2 ? kb[1].x : kb[1].y,
-                                jj == 0 ? ka[2].x : jj == 1 ? ka[2].y : jj == 2 ? kb[2].x : kb[2].y};
             PairOut<R_t> o;
-            ion_pair_nb<PREC, MEAS, IMGK>(fa, pi, pjv, ((m >> jj) & 1u) != 0, k, o);
+            if constexpr (TILEIMG) {
+                ion_pair_tile<PREC, MEAS>(fa, pit, pjv, ((m >> jj) & 1u) != 0, o);
+            } else {
+                const float k[3] = {jj == 0 ? ka[0].x : jj == 1 ? ka[0].y : jj == 2 ? kb[0].x : kb[0].y,
+                                    jj == 0 ? ka[1].x : jj == 1 ? ka[1].y : jj == 2 ? kb[1].x : kb[1].y,
+                                    jj == 0 ? ka[2].x : jj == 1 ? ka[2].y : jj == 2 ? kb[2].x : kb[2].y};
+                ion_pair_nb<PREC, MEAS, IMGK>(fa, pi, pjv, ((m >> jj) & 1u) != 0, k, o);
+            }
             if constexpr (PREC == PREC_FP64) acc.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
             else gs.add(o, SIM == SIM_MIX ? (R_t)pjv.w : (R_t)1);
             const R_t fsj = o.fs * wi;               // 0 unless the pair interacts
@@ -800,6 +814,47 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
                             pair_group_lo<SIM, MEAS, true>(fa, si, nli, z, z, wi, tlf, tll, 4 * (__ffs(gm) - 1),
                                                            jlim, diag, active, tid, sw, acc, my_acc);
                     }
+                }
+            }
+        } else if (IMGK && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+            // ions whose screen image integers are exact: the tile image
+            // when the tile has one, else each pair's own
+            if constexpr (IMGK && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+                int kcode = -1;
+                unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
+                const bool full = !diag && jlim == PB && all_active;
+                if (box.tile_img && kcode >= 0) {
+                    float2 th[3];
+                    const float nh[3] = {si.nx, si.ny, si.nz};
+                    const double pc[3] = {pi.x, pi.y, pi.z};
+                    double pt[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float k = img_of(kcode, c);
+                        const float h = fmaf(-k, fa.Lh[c], nh[c]);       // exact
+                        th[c] = make_float2(h, h);
+                        pt[c] = __fma_rn((double)k, fa.xl[c], pc[c]);
+                    }
+                    const double4 pit = make_double4(pt[0], pt[1], pt[2], pi.w);
+                    if (full) {
+                        for (; gm; gm &= gm - 1)
+                            pair_group<SIM, PREC, MEAS, false, true, true>(fa, pi, si, wi, tl, tlf,
+                                                                           4 * (__ffs(gm) - 1), jlim, diag, active,
+                                                                           tid, sw, acc, my_acc, th, pit);
+                    } else {
+                        for (; gm; gm &= gm - 1)
+                            pair_group<SIM, PREC, MEAS, true, true, true>(fa, pi, si, wi, tl, tlf,
+                                                                          4 * (__ffs(gm) - 1), jlim, diag, active,
+                                                                          tid, sw, acc, my_acc, th, pit);
+                    }
+                } else if (full) {
+                    for (; gm; gm &= gm - 1)
+                        pair_group<SIM, PREC, MEAS, false, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                                                                 diag, active, tid, sw, acc, my_acc);
+                } else {
+                    for (; gm; gm &= gm - 1)
+                        pair_group<SIM, PREC, MEAS, true, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                                                                diag, active, tid, sw, acc, my_acc);
                 }
             }
         } else {
