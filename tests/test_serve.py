@@ -20,14 +20,16 @@ def test_footprint_grows_with_n():
     small, big = footprint_bytes(1000), footprint_bytes(100000)
     assert big > 100 * small
     # half-pair scratch dominates at large n: the source-side partials take
-    # n^2/128 * 12 bytes, the target-side partials up to a quarter more
+    # n^2/128 * 12 bytes (FP64 rows), the target-side partials up to a
+    # quarter more; the mixed form's FP32 rows take half
     n = 131072
     assert n ** 2 / 128 * 12 < footprint_bytes(n) < 1.4 * n ** 2 / 128 * 12
+    assert n ** 2 / 128 * 6 < footprint_bytes(n, abi.YK_PREC_MIXED) < 0.85 * n ** 2 / 128 * 12
 
 
 def test_admission_passes_a_blocked_head():
     ws = [configs.pure_ion(n, 8, 16, 1.0, 175.0, seed=n) for n in (500, 4000, 800, 300)]
-    reqs = [Request(i, w, 100) for i, w in enumerate(ws)]
+    reqs = [Request(i, w, 100, abi.YK_PREC_FP64) for i, w in enumerate(ws)]
     budget = footprint_bytes(500) + footprint_bytes(4000) + footprint_bytes(800) // 2
     got, used = admit(reqs, 0, budget)
     assert [r.rid for r in got] == [0, 1, 3]       # 800 does not fit; 300 passes it

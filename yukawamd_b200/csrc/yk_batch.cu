@@ -69,7 +69,7 @@ struct RepDesc {
     int S;              // first slot (multiple of 128)
     int T;              // tiles
     int nseg;           // Si rows per target block
-    long long Sj_off;   // doubles
+    long long Sj_off;   // values (row_t of the batch's form)
     long long Si_off;   // doubles
     long long A;        // first double of the box's a(3,0:n+2) = 3 P
     int sm_off;         // first Sm row
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(PB, (pairs_ctas_per_sm<PREC, LO>()))
 k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ posf,
                     const int4* __restrict__ jobs, const int* __restrict__ njobs_p, int* __restrict__ counter,
                     const RepDesc* __restrict__ rd, const int* __restrict__ left, double* __restrict__ Si,
-                    double* __restrict__ Sj, double* __restrict__ Sm, unsigned* __restrict__ err)
+                    row_t<PREC>* __restrict__ Sj, double* __restrict__ Sm, unsigned* __restrict__ err)
 {
     __shared__ __align__(128) PairSmem<row_t<PREC>> sm;
     __shared__ __align__(16) ForceArgs sfa;
@@ -252,10 +252,10 @@ k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ p
 // Per slot of the boxes in sel (all if NULL) whose budget is not spent: the
 // fixed-order sum of its partials, the reference's scaling, and the store to
 // the caller's order (as k_combine).  tile_rep: box of every tile, -1 unused.
-template <int SIM>
+template <int SIM, int PREC>
 __global__ void __launch_bounds__(256)
 k_b_combine(const int* __restrict__ tile_rep, const RepDesc* __restrict__ rd, const int* __restrict__ sel,
-            const int* __restrict__ left, const double* __restrict__ Si, const double* __restrict__ Sj,
+            const int* __restrict__ left, const double* __restrict__ Si, const row_t<PREC>* __restrict__ Sj,
             const int* __restrict__ perm, const double* __restrict__ zii, const double* __restrict__ aii,
             double* __restrict__ a, int total_slots)
 {
@@ -276,9 +276,9 @@ k_b_combine(const int* __restrict__ tile_rep, const RepDesc* __restrict__ rd, co
         F[1] += e[1];
         F[2] += e[2];
     }
-    const double* sj = Sj + d->Sj_off + ((size_t)tri_index(R, 0) * PB + l) * 3;
+    const row_t<PREC>* sj = Sj + d->Sj_off + ((size_t)tri_index(R, 0) * PB + l) * 3;
     for (int R2 = 0; R2 <= R; ++R2) {
-        const double* e = sj + (size_t)R2 * PB * 3;
+        const row_t<PREC>* e = sj + (size_t)R2 * PB * 3;
         F[0] += e[0];
         F[1] += e[1];
         F[2] += e[2];
@@ -403,7 +403,8 @@ struct yk_batch {
     int* counter = nullptr;
     int* tile_rep = nullptr;
     int2* vblocks = nullptr;
-    double *Si = nullptr, *Sj = nullptr, *Sm = nullptr, *kpart = nullptr;
+    double *Si = nullptr, *Sm = nullptr, *kpart = nullptr;
+    void* Sj = nullptr;             // source-side rows: double (FP64) or float (mixed)
     DevScalars* ds = nullptr;
     unsigned* err = nullptr;
     double* series = nullptr;
@@ -481,15 +482,18 @@ static int launch_force_b(yk_batch* b, bool sel_new)
     if constexpr (PREC == PREC_MIXED) {
         if (b->all_lo) {
             k_force_pairs_batch<SIM, PREC, MEAS, true><<<b->force_grid_lo, PB, 0, b->stream>>>(
-                b->pos, b->posf, jobs, njp, b->counter, b->rd, b->left, b->Si, b->Sj, b->Sm, b->err);
+                b->pos, b->posf, jobs, njp, b->counter, b->rd, b->left, b->Si, static_cast<row_t<PREC>*>(b->Sj),
+                b->Sm, b->err);
             launched = true;
         }
     }
     if (!launched)
         k_force_pairs_batch<SIM, PREC, MEAS><<<b->force_grid, PB, 0, b->stream>>>(
-            b->pos, b->posf, jobs, njp, b->counter, b->rd, b->left, b->Si, b->Sj, b->Sm, b->err);
-    k_b_combine<SIM><<<(b->tcap * PB + 255) / 256, 256, 0, b->stream>>>(b->tile_rep, b->rd, sel_new ? b->sel : nullptr,
-                                                                 b->left, b->Si, b->Sj, b->perm, b->zii, b->aii,
+            b->pos, b->posf, jobs, njp, b->counter, b->rd, b->left, b->Si, static_cast<row_t<PREC>*>(b->Sj),
+            b->Sm, b->err);
+    k_b_combine<SIM, PREC><<<(b->tcap * PB + 255) / 256, 256, 0, b->stream>>>(b->tile_rep, b->rd, sel_new ? b->sel : nullptr,
+                                                                 b->left, b->Si, static_cast<row_t<PREC>*>(b->Sj),
+                                                                 b->perm, b->zii, b->aii,
                                                                  b->a, b->tcap * PB);
     return 2;
 }
@@ -1005,7 +1009,8 @@ static int create_empty(int sim, int prec_api, int nslots, long long max_units, 
                                              (int*)nullptr, (int*)nullptr, b->ucap, nslots, (int*)nullptr,
                                              (int*)nullptr, 0, b->key_bits);
     const long long U = max_units, S = max_tiles * PB;
-    const size_t need = sizeof(double) * (size_t)(14 * U + b->sj_cap + jb * PB * 3 + NSCAL * jb +
+    const size_t sj_elem = b->prec == PREC_MIXED ? sizeof(float) : sizeof(double);
+    const size_t need = sj_elem * (size_t)b->sj_cap + sizeof(double) * (size_t)(14 * U + jb * PB * 3 + NSCAL * jb +
                                                   (long long)NKIN * b->vb_cap) +
                         sizeof(double4) * S + sizeof(float) * (SHADOW_FLOATS / SHADOW_TILE) * S +
                         sizeof(int) * (4 * U + S + max_tiles) + sizeof(unsigned) * 2 * U + cub_bytes +
@@ -1056,7 +1061,11 @@ static int create_empty(int sim, int prec_api, int nslots, long long max_units, 
     BALLOC(b->counter, 1);
     BALLOC(b->tile_rep, max_tiles);
     BALLOC(b->vblocks, b->vb_cap);
-    BALLOC(b->Sj, b->sj_cap);
+    if (cudaMallocAsync(&b->Sj, (b->prec == PREC_MIXED ? sizeof(float) : sizeof(double)) * (size_t)b->sj_cap,
+                        b->stream) != cudaSuccess) {
+        yk_batch_destroy(b);
+        return bfail(nullptr, YK_ERR_NOMEM, "device allocation of Sj failed");
+    }
     BALLOC(b->kpart, (long long)NKIN * b->vb_cap);
     BALLOC(b->ds, nslots);
     BALLOC(b->err, 1);

@@ -134,7 +134,8 @@ struct yk_ctx {
     DevScalars* h_ds = nullptr;
     unsigned* h_err = nullptr;
     // half-pair kernel
-    double *Si = nullptr, *Sj = nullptr, *Sm = nullptr;
+    double *Si = nullptr, *Sm = nullptr;
+    void* Sj = nullptr;                 // source-side rows: double (FP64 form) or float (mixed form)
     int4* jobs = nullptr;
     int* row_slots = nullptr;
     int* job_counter = nullptr;
@@ -388,17 +389,23 @@ static int pair_ctas(int dev)
     return 6 * sms;
 }
 
-static size_t pair_scratch_bytes(int n, int seg, int dev)
+// Bytes of one source-side (Sj) value: the row type of the form.
+static size_t sj_elem_bytes(int precision)
+{
+    return precision == YK_PREC_MIXED ? sizeof(float) : sizeof(double);
+}
+
+static size_t pair_scratch_bytes(int n, int seg, int dev, int precision)
 {
     const int M = (n + PB - 1) / PB;
-    const size_t sj_bytes = sizeof(double) * ((size_t)M * (M + 1) / 2) * PB * 3;
+    const size_t sj_bytes = sj_elem_bytes(precision) * ((size_t)M * (M + 1) / 2) * PB * 3;
     if (sj_bytes > PAIR_SCRATCH_BUDGET) return sj_bytes;       // too large anyway: skip the job list
     std::vector<int4> jobs;
     std::vector<int> slots;
     build_pair_jobs(M, seg, pair_ctas(dev), jobs, slots);
     const size_t nseg = M > 0 ? (size_t)*std::max_element(slots.begin(), slots.end()) : 0;
     const size_t units = (size_t)M * (M + 1) / 2;
-    return sizeof(double) * (units * PB * 3 + (size_t)M * nseg * PB * 3 + jobs.size() * NSCAL) +
+    return sj_bytes + sizeof(double) * ((size_t)M * nseg * PB * 3 + jobs.size() * NSCAL) +
            sizeof(int4) * jobs.size() + sizeof(int) * (size_t)M;
 }
 
@@ -408,7 +415,8 @@ static void free_pairs(yk_ctx* c)
     cudaFree(c->Sj);
     cudaFree(c->Sm);
     cudaFree(c->jobs);
-    c->Si = c->Sj = c->Sm = nullptr;
+    c->Si = c->Sm = nullptr;
+    c->Sj = nullptr;
     c->jobs = nullptr;
     cudaFree(c->row_slots);
     c->row_slots = nullptr;
@@ -427,7 +435,7 @@ static int setup_pairs(yk_ctx* c)
     build_pair_jobs(M, c->seg, pair_ctas(c->dev), jobs, slots);
     const int nseg = M > 0 ? *std::max_element(slots.begin(), slots.end()) : 0;
     const size_t units = (size_t)M * (M + 1) / 2;
-    CK(c, cudaMalloc((void**)&c->Sj, sizeof(double) * units * PB * 3));
+    CK(c, cudaMalloc(&c->Sj, sj_elem_bytes(c->p.precision) * units * PB * 3));
     CK(c, cudaMalloc((void**)&c->Si, sizeof(double) * (size_t)M * nseg * PB * 3));
     CK(c, cudaMalloc((void**)&c->Sm, sizeof(double) * jobs.size() * NSCAL));
     CK(c, cudaMalloc((void**)&c->jobs, sizeof(int4) * jobs.size()));
@@ -450,7 +458,7 @@ static int resolve_kernel(yk_ctx* c)
     // autotuner candidate: with nucleons in species-major slot order it is
     // 1.35x slower than kernel 2 on the 51,200-nucleon box, and on the
     // 55,296-ion mixture 1.5x slower.)
-    if (k == 0) k = (pair_scratch_bytes(c->n, c->seg, c->dev) <= PAIR_SCRATCH_BUDGET) ? 2 : 1;
+    if (k == 0) k = (pair_scratch_bytes(c->n, c->seg, c->dev, c->p.precision) <= PAIR_SCRATCH_BUDGET) ? 2 : 1;
     if (k == 2 || k == 3) {
         int rc = setup_pairs(c);
         if (rc) return rc;
@@ -543,25 +551,25 @@ static int launch_force_t(yk_ctx* c)
     if (c->kernel == 3) {
         const int grid = persistent_grid<k_force_near<SIM, PREC, MEAS>>(c->dev);
         k_force_near<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-            c->pos, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+            c->pos, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
     } else if (lo_path<SIM, PREC>(c->fa)) {
         if constexpr (PREC == PREC_MIXED) {
             const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(c->dev);
             k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
         }
     } else if (SIM != SIM_NUCLEON && c->fa.img_k) {
         if constexpr (SIM != SIM_NUCLEON) {
             const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, false, true>>(c->dev);
             k_force_pairs<SIM, PREC, MEAS, false, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
         }
     } else {
         const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS>>(c->dev);
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-            c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, c->Sj, c->Sm, c->err);
+            c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
     }
-    k_combine<SIM><<<c->pj.M, COMB_THREADS, 0, c->stream>>>(c->Si, c->Sj, c->pj, c->perm, c->zii,
+    k_combine<SIM, PREC><<<c->pj.M, COMB_THREADS, 0, c->stream>>>(c->Si, static_cast<row_t<PREC>*>(c->Sj), c->pj, c->perm, c->zii,
                                                               c->aii, c->fa, c->a);
     return 2;
 }
@@ -924,7 +932,7 @@ int yk_create(const yk_params* p, int n, const double* x, const double* v, const
     size_t bytes = sizeof(double) * (3 * (size_t)n * 3 + 3 * (size_t)(n + 3) + 2 * (size_t)n) +
                    (sizeof(double4) + sizeof(float) * SHADOW_FLOATS / SHADOW_TILE) * ((size_t)n + SHADOW_TILE) + sizeof(int) * 5 * (size_t)n + cub_bytes +
                    sizeof(double) * (size_t)(8 * c->nfb + NKIN * c->nvb) + 4096;
-    const size_t pair_bytes = pair_scratch_bytes(n, c->seg, c->dev);
+    const size_t pair_bytes = pair_scratch_bytes(n, c->seg, c->dev, p->precision);
     const bool pairs_fit = pair_bytes <= PAIR_SCRATCH_BUDGET;
     if (pairs_fit) bytes += pair_bytes;
     size_t free_b = 0, total_b = 0;
@@ -1604,9 +1612,10 @@ static NoallocLayout noalloc_layout(int n)
 
 template <int SIM, int PREC, bool MEAS>
 static void noalloc_force(int dev, cudaStream_t st, const double4* pos, const float* posf, PairJobs pj,
-                          int* counter, const ForceArgs& fa, double* Si, double* Sj, double* Sm, unsigned* err,
+                          int* counter, const ForceArgs& fa, double* Si, void* Sj_v, double* Sm, unsigned* err,
                           const int* perm, const double* zii, const double* aii, double* a)
 {
+    row_t<PREC>* Sj = static_cast<row_t<PREC>*>(Sj_v);
     if (lo_path<SIM, PREC>(fa)) {
         if constexpr (PREC == PREC_MIXED) {
             const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(dev);
@@ -1618,13 +1627,13 @@ static void noalloc_force(int dev, cudaStream_t st, const double4* pos, const fl
         k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, pj.njobs), PB, 0, st>>>(pos, posf, pj, counter, fa, Si,
                                                                                 Sj, Sm, err);
     }
-    k_combine<SIM><<<pj.M, COMB_THREADS, 0, st>>>(Si, Sj, pj, perm, zii, aii, fa, a);
+    k_combine<SIM, PREC><<<pj.M, COMB_THREADS, 0, st>>>(Si, Sj, pj, perm, zii, aii, fa, a);
 }
 
 template <int SIM>
 static void noalloc_force_s(bool mixed, bool meas, int dev, cudaStream_t st, const double4* pos,
                             const float* posf, PairJobs pj, int* counter, const ForceArgs& fa, double* Si,
-                            double* Sj, double* Sm, unsigned* err, const int* perm, const double* zii,
+                            void* Sj, double* Sm, unsigned* err, const int* perm, const double* zii,
                             const double* aii, double* a)
 {
     if (mixed) {
@@ -1679,7 +1688,7 @@ extern "C" int yk_accel_noalloc(const yk_params* p, int n, const double* x_dev, 
     int* perm = reinterpret_cast<int*>(b + L.perm);
     int* iperm = reinterpret_cast<int*>(b + L.iperm);
     double* Si = reinterpret_cast<double*>(b + L.Si);
-    double* Sj = reinterpret_cast<double*>(b + L.Sj);
+    void* Sj = b + L.Sj;
     double* Sm = reinterpret_cast<double*>(b + L.Sm);
     int4* jobs = reinterpret_cast<int4*>(b + L.jobs);
     int* row_slots = reinterpret_cast<int*>(b + L.row_slots);

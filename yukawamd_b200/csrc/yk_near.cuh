@@ -240,10 +240,10 @@ __device__ __forceinline__ bool near_job(NearSmem& sm, const ForceArgs& fa, cons
                 v[2] += sm.sacc[w][e][2];
             }
         }
-        double* dj = bx.Sj + ((size_t)tri_index(C, R) * PB + tid) * 3;
-        dj[0] = v[0];
-        dj[1] = v[1];
-        dj[2] = v[2];
+        row_t<PREC>* dj = static_cast<row_t<PREC>*>(bx.Sj) + ((size_t)tri_index(C, R) * PB + tid) * 3;
+        dj[0] = (row_t<PREC>)v[0];
+        dj[1] = (row_t<PREC>)v[1];
+        dj[2] = (row_t<PREC>)v[2];
     }
     // target-side partial of job (R, s)
     double* di = bx.Si + (((size_t)R * bx.nseg_max + sg) * PB + tid) * 3;
@@ -263,7 +263,7 @@ __device__ __forceinline__ bool near_job(NearSmem& sm, const ForceArgs& fa, cons
 template <int SIM, int PREC, bool MEAS>
 __global__ void __launch_bounds__(PB, 5)
 k_force_near(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ job_counter, ForceArgs fa,
-             double* __restrict__ Si, double* __restrict__ Sj, double* __restrict__ Sm,
+             double* __restrict__ Si, row_t<PREC>* __restrict__ Sj, double* __restrict__ Sm,
              unsigned* __restrict__ err)
 {
     __shared__ __align__(128) NearSmem sm;

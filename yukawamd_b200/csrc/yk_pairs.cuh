@@ -648,7 +648,7 @@ struct BoxView {
     const double4* pos;
     const float* posf;
     double* Si;
-    double* Sj;
+    void* Sj;                      // source-side rows, row_t of the form
     int n, M, nseg_max;
 };
 
@@ -878,13 +878,16 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
         if (last) {
             __threadfence_block();
             if (lane == 0) sm.done[st] = 0;
-            double* dj = bx.Sj + (size_t)tri_index(C, R) * PB * 3;
+            // the unit's source-side row: FP64 in the FP64 form, FP32 (one
+            // rounding of the four warps' FP32 rows summed in FP64) in the
+            // mixed form
+            row_t<PREC>* dj = static_cast<row_t<PREC>*>(bx.Sj) + (size_t)tri_index(C, R) * PB * 3;
 #pragma unroll 4
             for (int k = lane; k < PB * 3; k += 32) {
                 double v = sm.acc_j[st][0][k];
 #pragma unroll
                 for (int w = 1; w < PWARPS; ++w) v += sm.acc_j[st][w][k];
-                dj[k] = v;
+                dj[k] = (row_t<PREC>)v;
             }
             __syncwarp();
             if (lane == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2, lo);
@@ -922,7 +925,7 @@ template <int SIM, int PREC, bool MEAS, bool LO = false, bool IMGK = false>
 __global__ void __launch_bounds__(PB, (pairs_ctas_per_sm<PREC, LO>()))
 k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, PairJobs pj,
               int* __restrict__ job_counter, ForceArgs fa, double* __restrict__ Si,
-              double* __restrict__ Sj, double* __restrict__ Sm, unsigned* __restrict__ err)
+              row_t<PREC>* __restrict__ Sj, double* __restrict__ Sm, unsigned* __restrict__ err)
 {
     __shared__ __align__(128) PairSmem<row_t<PREC>> sm;
     pairs_smem_init(sm);
@@ -959,9 +962,9 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
 constexpr int COMB_GROUPS = 2;
 constexpr int COMB_THREADS = COMB_GROUPS * PB * 3;
 
-template <int SIM>
+template <int SIM, int PREC>
 __global__ void __launch_bounds__(COMB_THREADS)
-k_combine(const double* __restrict__ Si, const double* __restrict__ Sj, PairJobs pj,
+k_combine(const double* __restrict__ Si, const row_t<PREC>* __restrict__ Sj, PairJobs pj,
           const int* __restrict__ perm, const double* __restrict__ zii,
           const double* __restrict__ aii, ForceArgs fa, double* __restrict__ a_out)
 {
@@ -974,9 +977,9 @@ k_combine(const double* __restrict__ Si, const double* __restrict__ Sj, PairJobs
     const int nseg = pj.row_slots[R];
 #pragma unroll 4
     for (int s = g; s < nseg; s += COMB_GROUPS) F += si[(size_t)s * ROW];
-    const double* sj = Sj + (size_t)tri_index(R, 0) * ROW + t;
+    const row_t<PREC>* sj = Sj + (size_t)tri_index(R, 0) * ROW + t;
 #pragma unroll 4
-    for (int R2 = g; R2 <= R; R2 += COMB_GROUPS) F += sj[(size_t)R2 * ROW];
+    for (int R2 = g; R2 <= R; R2 += COMB_GROUPS) F += (double)sj[(size_t)R2 * ROW];
     part[g][t] = F;
     __syncthreads();
     const int l = threadIdx.x;

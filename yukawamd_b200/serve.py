@@ -48,12 +48,17 @@ from ._lib import EngineError
 from .engine import SlotBatch
 
 PB = 128
-# device bytes per half-pair unit of a group's reserved scratch: the
-# source-side row (128 x 3 doubles) plus the target-side rows and job
-# entries at the default segment length (at most a quarter more)
-UNIT_BYTES = 3 * 8 * PB * 5 // 4 + 64
 # device bytes per particle of a group's reserved state and slot arrays
 PARTICLE_BYTES = 300
+
+
+def unit_bytes(precision=abi.YK_PREC_FP64):
+    """Device bytes per half-pair unit of reserved scratch: the source-side
+    row (128 x 3 values: doubles in the FP64 form, floats in the mixed form)
+    plus the target-side rows (doubles) and job entries at the default
+    segment length (a quarter of a double row at most) and slack."""
+    sj = 3 * PB * (4 if precision == abi.YK_PREC_MIXED else 8)
+    return sj + 3 * PB * 8 // 4 + 64
 
 
 def pair_units(n):
@@ -61,11 +66,11 @@ def pair_units(n):
     return t * (t + 1) // 2
 
 
-def footprint_bytes(n):
+def footprint_bytes(n, precision=abi.YK_PREC_FP64):
     """Device bytes a run of n particles takes inside a group: its state
     and slot arrays plus its half-pair scratch."""
     t = (int(n) + PB - 1) // PB
-    return PARTICLE_BYTES * (n + 3) + 84 * PB * t + UNIT_BYTES * pair_units(n)
+    return PARTICLE_BYTES * (n + 3) + 84 * PB * t + unit_bytes(precision) * pair_units(n)
 
 
 @dataclass
@@ -130,7 +135,7 @@ def admit(waiting, active_bytes, budget):
     used = [active_bytes]
 
     def fits(r):
-        need = footprint_bytes(r.n)
+        need = footprint_bytes(r.n, r.precision)
         if used[0] + need > budget:
             return False
         used[0] += need
@@ -153,7 +158,7 @@ class Group:
         self.chunk = chunk
         self.max_particles = max(PB, int(0.05 * budget_bytes) // PARTICLE_BYTES)
         part_bytes = PARTICLE_BYTES * self.max_particles
-        self.max_units = max(1, (budget_bytes - part_bytes) // UNIT_BYTES)
+        self.max_units = max(1, (budget_bytes - part_bytes) // unit_bytes(key[1]))
         self.batch = SlotBatch(proto, nslots, self.max_particles, self.max_units, device=device)
         if autotune:
             from . import tune
