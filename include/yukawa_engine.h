@@ -307,6 +307,12 @@ typedef struct yk_tuning {
                              list); 0 = automatic (8 FP64, 4 mixed)         */
     int sort_every;       /* steps between Hilbert re-orderings (-1 = never)  */
     int graph_steps;      /* steps captured per CUDA graph by yk_run          */
+    int source_split;     /* CTAs of the half-pair kernel (2, or auto when it
+                             picks 2) that share one 128-target block, each
+                             taking a contiguous 1/split of every source tile,
+                             so split x more CTAs (threads per target) work on
+                             a small box: 1, 2 or 4 (jobs of one tile then);
+                             0 = 1; ignored by kernels 1 and 3.  Batches: 0/1 */
 } yk_tuning;
 
 YK_API int yk_get_tuning(yk_ctx* ctx, yk_tuning* out);

@@ -68,7 +68,9 @@ KERNELS = {"rows": dict(force_kernel=abi.KERNEL_ROWS),
            "pairs": dict(force_kernel=abi.KERNEL_PAIRS),
            "pairs-unsorted-seg3": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, pair_seg=3),
            "near": dict(force_kernel=abi.KERNEL_NEAR),
-           "near-unsorted-seg3": dict(force_kernel=abi.KERNEL_NEAR, sort_every=-1, pair_seg=3)}
+           "near-unsorted-seg3": dict(force_kernel=abi.KERNEL_NEAR, sort_every=-1, pair_seg=3),
+           "pairs-split2": dict(force_kernel=abi.KERNEL_PAIRS, source_split=2),
+           "pairs-split4-unsorted": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, source_split=4)}
 
 
 @pytest.mark.parametrize("kern", list(KERNELS))
@@ -79,7 +81,7 @@ def test_accel_matches_oracle(gpu, orc, kind, n, meas, prec, kern):
     check_accel(orc, workload(kind, n, 100 + n), prec, meas, tuning=KERNELS[kern])
 
 
-@pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
+@pytest.mark.parametrize("kern", ["rows", "pairs", "near", "pairs-split4-unsorted"])
 @pytest.mark.parametrize("n", [1, 2, 3, 17, 127, 128, 129, 255, 257])
 @pytest.mark.parametrize("kind", ["pure", "mix", "nn"])
 def test_ragged_sizes(gpu, orc, kind, n, kern):

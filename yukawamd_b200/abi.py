@@ -112,6 +112,7 @@ class YkTuning(C.Structure):
         ("pair_seg", C.c_int),
         ("sort_every", C.c_int),
         ("graph_steps", C.c_int),
+        ("source_split", C.c_int),
     ]
 
 

@@ -148,6 +148,7 @@ struct yk_ctx {
     int kernel = 2;                 // 1 rows, 2 pairs, 3 near lists (resolved, never 0)
     int kernel_req = 0;             // as requested (0 = auto)
     int seg = DEFAULT_SEG;
+    int split = 1;                  // CTAs per unit of the half-pair kernel (yk_tuning.source_split)
     bool seg_auto = true;           // pair_seg not set by the caller: the precision's default
     int sort_every = DEFAULT_SORT_EVERY;
     int graph_steps = DEFAULT_GRAPH_STEPS;
@@ -375,6 +376,23 @@ static void build_pair_jobs(int M, int smax, int P, std::vector<int4>& jobs, std
     }
 }
 
+// Jobs of the half-pair kernel when `split` CTAs share every unit: each unit
+// (R, C) becomes `split` one-tile jobs, job `part` taking sources
+// [part 128/split, (part+1) 128/split) of tile C and writing its own Si slot
+// of row R.  The slot field carries the window: bits 0-19 the Si slot, 20-23
+// the part, 24-27 log2(split).  Longest rows first.
+static void build_split_jobs(int M, int split, std::vector<int4>& jobs, std::vector<int>& row_slots)
+{
+    jobs.clear();
+    row_slots.assign(M, 0);
+    int lg = 0;
+    while ((1 << lg) < split) ++lg;
+    for (int R = 0; R < M; ++R)
+        for (int C = R; C < M; ++C)
+            for (int part = 0; part < split; ++part)
+                jobs.push_back(make_int4(R, C, C + 1, row_slots[R]++ | (part << 20) | (lg << 24)));
+}
+
 static int auto_pair_seg(const yk_ctx* c)
 {
     return c->p.precision == YK_PREC_MIXED ? DEFAULT_SEG_MIXED : DEFAULT_SEG_FP64;
@@ -432,7 +450,9 @@ static int setup_pairs(yk_ctx* c)
     if (c->seg_auto) c->seg = auto_pair_seg(c);
     std::vector<int4> jobs;
     std::vector<int> slots;
-    build_pair_jobs(M, c->seg, pair_ctas(c->dev), jobs, slots);
+    // the near-list kernel reads whole tiles: no split for it
+    if (c->split > 1 && c->kernel_req != 3) build_split_jobs(M, c->split, jobs, slots);
+    else build_pair_jobs(M, c->seg, pair_ctas(c->dev), jobs, slots);
     const int nseg = M > 0 ? *std::max_element(slots.begin(), slots.end()) : 0;
     const size_t units = (size_t)M * (M + 1) / 2;
     CK(c, cudaMalloc(&c->Sj, sj_elem_bytes(c->p.precision) * units * PB * 3));
@@ -1034,6 +1054,7 @@ int yk_get_tuning(yk_ctx* c, yk_tuning* out)
     out->pair_seg = c->seg;
     out->sort_every = c->sort_every;
     out->graph_steps = c->graph_steps;
+    out->source_split = c->kernel == 2 ? c->split : 1;
     return YK_OK;
 }
 
@@ -1043,6 +1064,9 @@ int yk_set_tuning(yk_ctx* c, const yk_tuning* t)
     if (t->force_kernel < 0 || t->force_kernel > 3) return fail(c, YK_ERR_ARG, "force_kernel must be 0..3");
     if (t->pair_seg < 0 || t->graph_steps < 0 || t->sort_every < -1)
         return fail(c, YK_ERR_ARG, "bad tuning values");
+    if (t->source_split != 0 && t->source_split != 1 && t->source_split != 2 && t->source_split != 4)
+        return fail(c, YK_ERR_ARG, "source_split must be 0, 1, 2 or 4");
+    c->split = t->source_split > 1 ? t->source_split : 1;
     CK(c, cudaSetDevice(c->dev));
     CK(c, cudaStreamSynchronize(c->stream));
     drop_graphs(c);

@@ -719,6 +719,11 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
     const int warp = tid >> 5, lane = tid & 31;
     const int n = bx.n;
     const int i = R * PB + tid;
+    // a unit shared by 2^lg jobs (source_split): this one takes sources
+    // [w0, w1) of every tile (multiples of 32)
+    const int lg = (sg >> 24) & 15, part = (sg >> 20) & 15;
+    sg &= 0xFFFFF;
+    const int w0 = (part * PB) >> lg, w1 = ((part + 1) * PB) >> lg;
     const bool active = i < n;
     const double4 pi = active ? bx.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
     const ScreenI si = load_screen_i(bx.posf, active ? i : 0);
@@ -750,7 +755,7 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
     for (int C = C0; C < C1; ++C, ++q) {
         const int st = q & 1;
         if (!mbar_wait_abortable(&sm.bar[st], (q >> 1) & 1u, err, &sm.abort)) break;
-        const int jlim = min(PB, n - C * PB);
+        const int jlim = min(min(PB, n - C * PB), w1);
         const bool diag = (C == R);
         const double4* tl = sm.tile[st];
         const float* tlf = sm.tilef[st];
@@ -759,13 +764,14 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
         for (int k = lane; k < PB * 3; k += 32) my_acc[k] = 0.0;
         __syncwarp();
         // on the diagonal tile only sources after the warp's first target count
-        const int jmin = diag ? 32 * warp + 1 : 0;
+        const int jmin = max(diag ? 32 * warp + 1 : 0, w0);
+        const bool full = !diag && jlim == PB && all_active && w0 == 0;
         if (lo) {
             if constexpr (PREC == PREC_MIXED && SIM == SIM_NUCLEON) {
                 unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
                 const float* tll = reinterpret_cast<const float*>(tl);
                 const double4* gsrc = bx.pos + (size_t)C * PB;
-                if (!diag && jlim == PB && all_active) {
+                if (full) {
                     for (; gm; gm &= gm - 1)
                         pair_group_nn_lo<MEAS, false>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
                                                       diag, active, tid, sw, acc, my_acc);
@@ -779,7 +785,6 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
                 int kcode = -1;
                 unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
                 const float* tll = reinterpret_cast<const float*>(tl);
-                const bool full = !diag && jlim == PB && all_active;
                 if (box.tile_img && kcode >= 0) {
                     // one image for the whole tile: fold it into the target
                     float2 th[3], tl2[3];
@@ -822,7 +827,6 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
             if constexpr (IMGK && (SIM == SIM_PURE || SIM == SIM_MIX)) {
                 int kcode = -1;
                 unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
-                const bool full = !diag && jlim == PB && all_active;
                 if (box.tile_img && kcode >= 0) {
                     float2 th[3];
                     const float nh[3] = {si.nx, si.ny, si.nz};
@@ -859,7 +863,7 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
             }
         } else {
             unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
-            if (!diag && jlim == PB && all_active) {
+            if (full) {
                 for (; gm; gm &= gm - 1)
                     pair_group<SIM, PREC, MEAS, false, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
                                                              diag, active, tid, sw, acc, my_acc);
@@ -882,8 +886,9 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
             // rounding of the four warps' FP32 rows summed in FP64) in the
             // mixed form
             row_t<PREC>* dj = static_cast<row_t<PREC>*>(bx.Sj) + (size_t)tri_index(C, R) * PB * 3;
+            // (only this job's window: the other parts of a split unit write the rest)
 #pragma unroll 4
-            for (int k = lane; k < PB * 3; k += 32) {
+            for (int k = 3 * w0 + lane; k < 3 * w1; k += 32) {
                 double v = sm.acc_j[st][0][k];
 #pragma unroll
                 for (int w = 1; w < PWARPS; ++w) v += sm.acc_j[st][w][k];

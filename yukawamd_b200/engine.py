@@ -171,10 +171,12 @@ class Engine:
         check(self._lib.yk_get_tuning(self._ctx, C.byref(t)), self._ctx)
         return t
 
-    def set_tuning(self, force_kernel=None, pair_seg=None, sort_every=None, graph_steps=None):
+    def set_tuning(self, force_kernel=None, pair_seg=None, sort_every=None, graph_steps=None,
+                   source_split=None):
         t = self.tuning()
         for name, val in (("force_kernel", force_kernel), ("pair_seg", pair_seg),
-                          ("sort_every", sort_every), ("graph_steps", graph_steps)):
+                          ("sort_every", sort_every), ("graph_steps", graph_steps),
+                          ("source_split", source_split)):
             if val is not None:
                 setattr(t, name, int(val))
         check(self._lib.yk_set_tuning(self._ctx, C.byref(t)), self._ctx)

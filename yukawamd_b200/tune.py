@@ -1,9 +1,11 @@
 """Autotuner for the engine's tunables.
 
-For one box the engine can run its force call two ways (the half-pair kernel
-with scratch, or the row kernel that evaluates each pair from both sides)
-and cap the half-pair jobs at `pair_seg` source tiles (the job list shrinks
-them towards its end); it refreshes
+For one box the engine can run its force call three ways (the half-pair
+kernel with scratch, the same over per-warp near-source lists, or the row
+kernel that evaluates each pair from both sides), cap the half-pair jobs at
+`pair_seg` source tiles (the job list shrinks them towards its end), let
+1, 2 or 4 CTAs share each 128-target block (`source_split`: the threads per
+target, for small boxes); it refreshes
 the Morton order every `sort_every` steps.  Which choice is fastest depends on
 N, the cutoff radius relative to the box, the interaction and the precision,
 so the tuner measures candidates on the caller's own workload (CUDA-event
@@ -32,7 +34,13 @@ CANDIDATES = [
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=20),
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=-1),
     dict(force_kernel=abi.KERNEL_ROWS, pair_seg=8, sort_every=50),
+    # threads per target: 2 or 4 CTAs share each 128-target block (small boxes)
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=50, source_split=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=50, source_split=4),
 ]
+# source_split > 1 makes one job per unit and part: only worth trying while the
+# box has few tiles (it is there to fill the GPU with a small box)
+SPLIT_MAX_N = 16384
 
 
 def cache_path():
@@ -93,10 +101,13 @@ def tune(engine, candidates=None, steps=6, warmup=2, device=0, save=True):
     """Time every candidate on this engine's workload; apply and return the
     best one.  The engine's positions are restored afterwards, so tuning does
     not advance the caller's trajectory."""
-    candidates = candidates or CANDIDATES
+    candidates = candidates or [c for c in CANDIDATES
+                                if c.get("source_split", 1) == 1 or engine.n <= SPLIT_MAX_N]
     x, v, vold, a = engine.get_state()
     results = []
     for cand in candidates:
+        cand = dict(cand)
+        cand.setdefault("source_split", 1)
         try:
             ms = measure(engine, cand, steps, warmup)
         except Exception as exc:          # e.g. scratch too large for this N
@@ -162,5 +173,6 @@ def apply(engine, device=0):
     ent = _load().get(key_for(engine, device))
     if not ent:
         return False
-    engine.set_tuning(**{k: ent[k] for k in ("force_kernel", "pair_seg", "sort_every") if k in ent})
+    engine.set_tuning(**{k: ent[k] for k in ("force_kernel", "pair_seg", "sort_every", "source_split")
+                         if k in ent})
     return True
