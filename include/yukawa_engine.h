@@ -66,11 +66,12 @@ extern "C" {
 /* ---- arithmetic of the pair terms -------------------------------------- */
 #define YK_PREC_FP64        0   /* all FP64: the drop-in form                    */
 #define YK_PREC_MIXED       1   /* FP64 positions, velocities and Verlet update;
-                                   FP32 displacement (ions: exact differences of
+                                   FP32 displacement (exact differences of
                                    grid-rounded coordinates plus a correction;
-                                   nucleons: the FP64 minimum image, cast) and
-                                   FP32 pair terms with compensated (two-sum)
-                                   accumulation                                 */
+                                   nucleon pairs within 2^-7 fm of |d| = L/2 on
+                                   an axis take the FP64 minimum image, cast)
+                                   and FP32 pair terms with compensated
+                                   (two-sum) accumulation                       */
 
 /* ---- integrators -------------------------------------------------------- */
 #define YK_VV1              1   /* vel_verlet_1.f: two half kicks              */

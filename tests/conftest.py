@@ -3,6 +3,12 @@ import sys
 
 import pytest
 
+# The oracle's mixture loops use schedule(runtime), as the reference does
+# (int_ion_mix.f:159,223); with OMP_SCHEDULE unset, libgomp schedules them
+# dynamically with chunks of one iteration, which makes a full-size call take
+# a minute.  Set before the oracle's OpenMP runtime is loaded.
+os.environ.setdefault("OMP_SCHEDULE", "static")
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
