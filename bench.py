@@ -82,6 +82,10 @@ def parse():
                     help="Poisson arrival rate (runs/s) of the served ensemble in the default line")
     ap.add_argument("--serve", action="store_true",
                     help="instead of the benchmark: serve a request stream and report latency")
+    ap.add_argument("--tune-report", action="store_true",
+                    help="instead of the benchmark: run the autotuner on the pure-ion OCP (N=4,096), the ion "
+                         "mixture (N=55,296), nucleons (N=51,200) and the 256-replica ensemble and report the "
+                         "candidates tried and the winners")
     ap.add_argument("--serve-ensemble", action="store_true",
                     help="instead of the benchmark: serve the 256-replica ensemble and report latency")
     ap.add_argument("--ensemble-serve-steps", type=int, default=1000)
@@ -663,6 +667,32 @@ def serve_ensemble(args, dist):
     return rep
 
 
+def tune_report(args, dist):
+    """The autotuner (yukawamd_b200/tune.py) on the benchmark workloads: for
+    each single box every candidate's force-call time (CUDA events) and the
+    winner; for the replica ensemble every job segment length's graph time."""
+    from yukawamd_b200 import abi, configs, tune
+    from yukawamd_b200.engine import Batch, Engine
+    out = {"metric": "autotuner: force-call ms per candidate (single boxes), graph ms per 50 steps (ensemble)"}
+    for name, w in (("ocp_4096", configs.pure_ion_ocp(1)), ("mix_55296", configs.ion_mixture_cfg(2)),
+                    ("nucleon_51200", configs.nucleon_matter(3))):
+        for prec in ("fp64", "mixed"):
+            p = abi.YK_PREC_MIXED if prec == "mixed" else abi.YK_PREC_FP64
+            with Engine(w, device=dist.local, precision=p) as e:
+                e.accel(True)
+                best, best_ms, res = tune.tune(e, device=dist.local, save=False)
+            out["%s_%s" % (name, prec)] = {
+                "winner": best, "force_ms": best_ms,
+                "tried": [[r[0] if r[0] != float("inf") else None, r[1]] for r in res]}
+    boxes = configs.replica_ensemble(4)
+    with Batch(boxes, device=dist.local, precision=abi.YK_PREC_MIXED) as b:
+        b.accel(True)
+        best, best_ms, tried = tune.tune_batch(b, steps=50, device=dist.local, save=False)
+    out["ensemble_256_mixed"] = {"winner": {"pair_seg": best}, "graph_ms_50_steps": best_ms,
+                                 "tried": [[ms, {"pair_seg": seg}] for ms, seg in tried]}
+    return out
+
+
 def run_reference(args):
     """The reference's CPU algorithm (OpenMP C restatement) on all host cores."""
     from oracle.oracle import Oracle
@@ -716,6 +746,11 @@ def main():
     dist = Dist()
     dist.init()
     try:
+        if args.tune_report:
+            out = tune_report(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(out), flush=True)
+            return 0
         if args.serve_ensemble:
             out = serve_ensemble(args, dist)
             if dist.rank == 0:

@@ -18,12 +18,12 @@
 // PREC_FP64: all FP64 (exp_neg_f64, our table-driven exp, and rsqrt() from
 // the CUDA math library; rsqrt replaces the reference's sqrt and divide,
 // 1/(r r^2) = rinv^3).
-// PREC_MIXED: the r^2, rsqrt, exp and force terms in FP32.  Ion pairs take
-// their displacement from the shadow's hi/lo parts (screen_d_x2: exact FP32
-// hi-part differences plus a lo correction, no FP64 arithmetic) and e^{-mu r}
-// from the hardware base-2 exponential (exp_neg_f32_xu) when the box allows
-// it (fa.lo); otherwise, and for nucleons, the displacement and minimum
-// image are FP64, then cast to FP32.
+// PREC_MIXED: the r^2, rsqrt, exp and force terms in FP32.  Pairs take their
+// displacement from the shadow's hi/lo parts (screen_d_x2: exact FP32 hi-part
+// differences plus a lo correction, no FP64 arithmetic) when the box allows it
+// (ions: fa.lo; nucleons: fa.hilo, with the pairs near |d| = L/2 on the FP64
+// minimum image) and e^{-mu r} from the hardware base-2 exponential;
+// otherwise the displacement and minimum image are FP64, then cast to FP32.
 //
 // Particles are addressed by "slot": the engine keeps them in a Morton
 // (space-filling-curve) order so that the 32 targets of a warp are close in
@@ -577,17 +577,24 @@ __device__ __forceinline__ void ion_pair_f32(const ForceArgs& fa, float r2, bool
 
 // ion_pair_f32's terms for two pairs at once (the FP32 arithmetic paired):
 // r2 their r^2, msk 1 for a pair that interacts and 0 otherwise.  Returns fs
-// (0 for a masked pair) and, when measuring, u and w.
+// (0 for a masked pair) and, when measuring, u and w.  e^{-mu r} is the
+// hardware base-2 exponential of the rounded product y = -mu r log2(e): the
+// rounding of y changes the result by at most |y| 2^-24 ln 2 relative, below
+// the instruction's own error (about 2 ulp) for the pairs that carry the
+// force (mu r of a few), and about 6e-7 at the cutoff mu r = 10, where the
+// term is weighted by e^-10; fs = q (1 + mu r) with q = e^{-mu r} / r^3.
 template <bool MEAS>
 __device__ __forceinline__ void ion_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2& fs, float2& u,
                                              float2& w)
 {
+    const float L2E = 1.44269502162933349609375f;           // float(log2 e)
     const float2 r2s = make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f);
     const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
     const float2 mr = __fmul2_rn(make_float2(fa.xmucf, fa.xmucf), __fmul2_rn(r2s, rinv));
-    const float2 er = __fmul2_rn(exp_neg_f32_xu_x2(mr), rinv);
-    const float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(make_float2(1.0f, 1.0f), mr), er), __fmul2_rn(rinv, rinv));
-    fs = __fmul2_rn(f, msk);
+    const float2 y = __fmul2_rn(mr, make_float2(-L2E, -L2E));
+    const float2 er = __fmul2_rn(make_float2(ex2_approx(y.x), ex2_approx(y.y)), rinv);
+    const float2 q = __fmul2_rn(er, __fmul2_rn(__fmul2_rn(rinv, rinv), msk));
+    fs = __ffma2_rn(mr, q, q);
     if constexpr (MEAS) {
         u = __fmul2_rn(__fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf)), msk);
         w = __fmul2_rn(fs, r2);

@@ -291,10 +291,16 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
     float2 fxa[3], fxb[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        fxa[c] = __fmul2_rn(ga, da[c]);
-        fxb[c] = __fmul2_rn(gb, db[c]);
-        const float2 sc = __fadd2_rn(fxa[c], fxb[c]);
-        gs.f[c] = -(sc.x + sc.y);
+        if constexpr (MEAS) {
+            // the products are kept for the pressure tensor
+            fxa[c] = __fmul2_rn(ga, da[c]);
+            fxb[c] = __fmul2_rn(gb, db[c]);
+            const float2 sc = __fadd2_rn(fxa[c], fxb[c]);
+            gs.f[c] = -(sc.x + sc.y);
+        } else {
+            const float2 sc = __ffma2_rn(gb, db[c], __fmul2_rn(ga, da[c]));
+            gs.f[c] = -(sc.x + sc.y);
+        }
     }
     if constexpr (MEAS) {
         const float2 su = __ffma2_rn(ub, wjb, __fmul2_rn(ua, wja));
