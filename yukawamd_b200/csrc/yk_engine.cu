@@ -56,6 +56,22 @@ __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b)
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// yk_set_state: flag a NaN or Inf among cnt staged values ...
+__global__ void k_check_finite(const double* __restrict__ p, size_t cnt, unsigned* __restrict__ flag)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool bad = i < cnt && !isfinite(p[i]);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+// ... and move them into the state only if none was flagged.
+__global__ void k_commit_state(const double* __restrict__ src, double* __restrict__ dst, size_t cnt,
+                               const unsigned* __restrict__ flag)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < cnt && *flag == 0) dst[i] = src[i];
+}
+
 // Failure path of the bounded waits (yk_wait_selftest): one CTA of 128
 // threads waits on an mbarrier that no copy is ever issued against, so its
 // phase 0 never completes.  Warps 0-1 wait as the pair kernels' warps do
@@ -124,6 +140,8 @@ struct yk_ctx {
     double *fpart = nullptr, *kpart = nullptr;
     double *vpart = nullptr, *vsums = nullptr;   // ttot / tnorm / cancel_vcom sums
     double* a_vtot = nullptr;                   // accelerations of yk_vtot (discarded)
+    double* stage = nullptr;                    // yk_set_state: x, v, vold, a as copied in, before the check
+    unsigned* nonfinite = nullptr;              // yk_set_state: set by k_check_finite
     unsigned long long* gofr = nullptr;         // yk_gofr_counts histogram
     int gofr_cap = 0;
     DevScalars* ds = nullptr;
@@ -422,7 +440,6 @@ static size_t pair_scratch_bytes(int n, int seg, int dev, int precision)
     std::vector<int> slots;
     build_pair_jobs(M, seg, pair_ctas(dev), jobs, slots);
     const size_t nseg = M > 0 ? (size_t)*std::max_element(slots.begin(), slots.end()) : 0;
-    const size_t units = (size_t)M * (M + 1) / 2;
     return sj_bytes + sizeof(double) * ((size_t)M * nseg * PB * 3 + jobs.size() * NSCAL) +
            sizeof(int4) * jobs.size() + sizeof(int) * (size_t)M;
 }
@@ -893,7 +910,8 @@ int yk_destroy(yk_ctx* c)
     void* bufs[] = {c->x, c->v, c->vold, c->a, c->zii, c->aii, c->pos, c->posf, c->perm, c->iperm,
                     c->keys0, c->keys1, c->idx0, c->cub_tmp, c->fpart, c->kpart, c->vpart, c->vsums,
                     c->ds, c->err,
-                    c->series, c->series_idx, c->job_counter, c->flush_buf, c->snap, c->a_vtot, c->gofr};
+                    c->series, c->series_idx, c->job_counter, c->flush_buf, c->snap, c->a_vtot, c->gofr,
+                    c->stage, c->nonfinite};
     for (void* b : bufs) cudaFree(b);
     if (c->snap_taken) cudaEventDestroy(c->snap_taken);
     if (c->snap_done) cudaEventDestroy(c->snap_done);
@@ -1310,22 +1328,45 @@ int yk_snapshot_begin(yk_ctx* c, double* x, double* v, double* a)
 int yk_set_state(yk_ctx* c, const double* x, const double* v, const double* vold, const double* a)
 {
     if (!c) return fail(nullptr, YK_ERR_ARG, "ctx is NULL");
-    const size_t cnt = 3 * (size_t)c->n;
-    if ((x && !all_finite(x, cnt)) || (v && !all_finite(v, cnt)) || (vold && !all_finite(vold, cnt)) ||
-        (a && !all_finite(a, cnt)))
-        return fail(c, YK_ERR_NONFINITE, "NaN or Inf in a state array");
     CK(c, cudaSetDevice(c->dev));
+    const size_t cnt = 3 * (size_t)c->n;
     const size_t b = sizeof(double) * cnt;
-    if (x) CK(c, cudaMemcpyAsync(c->x, x, b, cudaMemcpyHostToDevice, c->stream));
-    if (v) CK(c, cudaMemcpyAsync(c->v, v, b, cudaMemcpyHostToDevice, c->stream));
-    if (vold) CK(c, cudaMemcpyAsync(c->vold, vold, b, cudaMemcpyHostToDevice, c->stream));
-    if (a) CK(c, cudaMemcpyAsync(c->a, a, b, cudaMemcpyHostToDevice, c->stream));
+    if (!c->stage) {
+        CK(c, cudaMalloc((void**)&c->stage, 4 * b));
+        CK(c, cudaMalloc((void**)&c->nonfinite, sizeof(unsigned)));
+    }
+    // The arrays are copied into a staging buffer and checked for NaN / Inf
+    // on the device; only if all are finite does k_commit_state move them
+    // into the state, so a rejected call leaves the state as it was.
+    const double* src[4] = {x, v, vold, a};
+    double* dst[4] = {c->x, c->v, c->vold, c->a};
+    CK(c, cudaMemsetAsync(c->nonfinite, 0, sizeof(unsigned), c->stream));
+    int k = 0;
+    for (int q = 0; q < 4; ++q) {
+        if (!src[q]) continue;
+        CK(c, cudaMemcpyAsync(c->stage + q * cnt, src[q], b, cudaMemcpyHostToDevice, c->stream));
+        k_check_finite<<<(int)((cnt + 255) / 256), 256, 0, c->stream>>>(c->stage + q * cnt, cnt, c->nonfinite);
+        ++k;
+    }
+    for (int q = 0; q < 4; ++q) {
+        if (!src[q]) continue;
+        k_commit_state<<<(int)((cnt + 255) / 256), 256, 0, c->stream>>>(c->stage + q * cnt, dst[q], cnt,
+                                                                         c->nonfinite);
+        ++k;
+    }
+    unsigned bad = 0;
+    CK(c, cudaMemcpyAsync(c->h_err, c->nonfinite, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    bad = *c->h_err;
+    *c->h_err = 0;
+    g_launches += k;
+    if (bad) return fail(c, YK_ERR_NONFINITE, "NaN or Inf in a state array");
     if (x) {
         // keep the current Morton order; the next scheduled sort refreshes it
         c->pos_dirty = true;
         g_launches += enqueue_order(c, false);
+        CK(c, cudaStreamSynchronize(c->stream));
     }
-    CK(c, cudaStreamSynchronize(c->stream));
     return YK_OK;
 }
 
