@@ -145,13 +145,20 @@ k_b_drift(const int2* __restrict__ vb, const RepDesc* __restrict__ rd, const int
     if (local >= s.n) return;
     const int gi = d->P + local;
     const double* ar = a + d->A;
+    // all nine loads before the first store (they are then in flight together)
+    double xi[3], vi[3], ai[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        xi[k] = x[3 * gi + k];
+        vi[k] = v[3 * gi + k];
+        ai[k] = ar[3 * local + k];
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const int e = 3 * gi + k;
-        const double vi = v[e], ai = ar[3 * local + k];
-        x[e] = drift1(x[e], vi, ai, s, k);
-        vold[e] = vi;
-        v[e] = __dadd_rn(vi, __dmul_rn(s.dt, ai));
+        x[e] = drift1(xi[k], vi[k], ai[k], s, k);
+        vold[e] = vi[k];
+        v[e] = __dadd_rn(vi[k], __dmul_rn(s.dt, ai[k]));
     }
 }
 
@@ -191,14 +198,21 @@ k_b_post(const int2* __restrict__ vb, const RepDesc* __restrict__ rd, const int*
     if (local < d->sa.n) {
         const int gi = d->P + local;
         const double* ar = a + d->A;
-        double vv[3];
+        double vv[3], vo[3], aa[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const double vp = __dadd_rn(vold[3 * gi + k], __dmul_rn(dt, ar[3 * local + k]));
-            vv[k] = __dmul_rn(0.5, __dadd_rn(v[3 * gi + k], vp));
+            vv[k] = v[3 * gi + k];
+            vo[k] = vold[3 * gi + k];
+            aa[k] = ar[3 * local + k];
+        }
+        const double am = aii[gi];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double vp = __dadd_rn(vo[k], __dmul_rn(dt, aa[k]));
+            vv[k] = __dmul_rn(0.5, __dadd_rn(vv[k], vp));
             v[3 * gi + k] = vv[k];
         }
-        kin_sums<KIN>(tk, aii[gi], vv[0], vv[1], vv[2]);
+        kin_sums<KIN>(tk, am, vv[0], vv[1], vv[2]);
     }
     if constexpr (KIN) block_sum_store<NKIN>(tk, red, kpart + (size_t)blockIdx.x * NKIN);
 }
@@ -206,7 +220,8 @@ k_b_post(const int2* __restrict__ vb, const RepDesc* __restrict__ rd, const int*
 // The persistent force kernel over the work items of jobs[0 .. *njobs); the
 // items of boxes whose step budget is spent are passed over.
 template <int SIM, int PREC, bool MEAS, bool LO = false>
-__global__ void __launch_bounds__(PB, (pairs_ctas_per_sm<PREC, LO>()))
+// (6 CTAs per SM for the mixed hi/lo form: at 7, the box descriptors spill)
+__global__ void __launch_bounds__(PB, (pairs_ctas_per_sm<SIM_MIX, PREC, LO>()))
 k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ posf,
                     const int4* __restrict__ jobs, const int* __restrict__ njobs_p, int* __restrict__ counter,
                     const RepDesc* __restrict__ rd, const int* __restrict__ left, double* __restrict__ Si,

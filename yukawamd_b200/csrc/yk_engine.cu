@@ -416,8 +416,8 @@ static int auto_pair_seg(const yk_ctx* c)
     return c->p.precision == YK_PREC_MIXED ? DEFAULT_SEG_MIXED : DEFAULT_SEG_FP64;
 }
 
-// Resident CTAs of the half-pair kernels on a device (the most any variant
-// runs per SM), for the job builder.
+// Resident CTAs of the half-pair kernels on a device (6 per SM), for the job
+// builder's job lengths.
 static int pair_ctas(int dev)
 {
     int sms = 148;
@@ -670,20 +670,22 @@ static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool resort, bool t
     if (resort || c->need_sort) k += enqueue_order(c, true);
     else if (c->pos_dirty) k += enqueue_order(c, false);
     const int nb = c->nvb;
+    const int nb3 = (int)((3LL * c->n + VBLOCK - 1) / VBLOCK);   // element-wise drifts
     cudaStream_t st = c->stream;
     const StepArgs& s = c->sa;
     switch (c->p.integrator) {
     case YK_VV1:
-        k_drift_vv1<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->iperm, c->pos, c->posf, s);
+        k_drift_vv1<<<nb3, VBLOCK, 0, st>>>(c->x, c->v, c->a, s);
         break;
     case YK_VV3:
-        k_drift_vv3<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->aii, c->iperm, c->pos, c->posf, s);
+        k_drift_vv3<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->a, c->zii, c->aii, s);
         break;
     default:
-        k_drift_vv2<<<nb, VBLOCK, 0, st>>>(c->x, c->v, c->vold, c->a, c->zii, c->iperm, c->pos, c->posf, s);
+        k_drift_vv2<<<nb3, VBLOCK, 0, st>>>(c->x, c->v, c->vold, c->a, s);
         break;
     }
-    ++k;
+    k_pack_slots<<<nb, VBLOCK, 0, st>>>(c->perm, c->x, c->zii, c->pos, c->posf, c->n, s.pack_w);
+    k += 2;
     k += enqueue_force(c, meas, timed);
     int kin_mode;
     switch (c->p.integrator) {

@@ -6,14 +6,16 @@
 //   vel_verlet_1.f:16-89   drift + wrap, v += dt/2 a, accel, v += dt/2 a
 //   vel_verlet_3.f:20-100  Spreiter-Walter magnetic Verlet
 //
-// Arrays keep the Fortran layout x(3,0:n-1): one thread per particle reads
-// and writes its three consecutive doubles.  Every element update uses
+// Arrays keep the Fortran layout x(3,0:n-1).  The VV1/VV2 drifts take one
+// thread per element (each warp access is 256 contiguous bytes); the kernels
+// that mix a particle's components take one thread per particle and load all
+// of its values before the first store.  Every element update uses
 // explicitly rounded operations (__dadd_rn / __dmul_rn) so that nothing is
 // contracted into an FMA: positions and velocities come out bit-identical to
 // the reference's arithmetic (which is compiled without FMA) given the same
-// accelerations.  The drift kernels also pack the FP64 positions with the
-// per-particle weight (zii) into the Morton-ordered double4 array the force
-// kernels stream (slot iperm[i] for particle i).
+// accelerations.  After a drift, k_pack_slots gathers the FP64 positions with
+// the per-particle weight (zii) into the slot-ordered double4 array and the
+// FP32 shadow that the force kernels stream.
 #pragma once
 
 #include "yk_force.cuh"
@@ -48,74 +50,72 @@ __device__ __forceinline__ void store_pos(double4* pos, float* posf, int slot, c
     store_shadow(posf, slot, xn[0], xn[1], xn[2], (float)w);
 }
 
+// The slot-ordered FP64 positions and FP32 shadow after a drift, a thread
+// per slot: the position is gathered through perm and each slot's words are
+// written in slot order (a warp writes contiguous runs).  The drift kernels
+// themselves only touch the caller-order arrays, all coalesced; writing the
+// slot copies from them would scatter every 4-byte shadow word through the
+// permutation, one 32-byte sector each.
+static __global__ void k_pack_slots(const int* __restrict__ perm, const double* __restrict__ x,
+                                    const double* __restrict__ zii, double4* __restrict__ pos,
+                                    float* __restrict__ posf, int n, int pack_w)
+{
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= n) return;
+    const int o = perm[sl];
+    const double xn[3] = {x[3 * o], x[3 * o + 1], x[3 * o + 2]};
+    store_pos(pos, posf, sl, xn, pack_w ? zii[o] : 0.0);
+}
+
 // x = x + v dt + afac a, wrapped once (vel_verlet_2.f:36-42)
 __device__ __forceinline__ double drift1(double x, double v, double a, const StepArgs& s, int k)
 {
     return wrap_once(__dadd_rn(__dadd_rn(x, __dmul_rn(v, s.dt)), __dmul_rn(s.afac, a)), s.xl[k]);
 }
 
-// VV2 first half: drift, vold = v, v += dt a.
+// VV2 first half: drift, vold = v, v += dt a; one thread per element
+// (component e % 3 of particle e / 3).
 static __global__ void k_drift_vv2(double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold,
-                            const double* __restrict__ a, const double* __restrict__ zii,
-                            const int* __restrict__ iperm, double4* __restrict__ pos,
-                            float* __restrict__ posf, StepArgs s)
+                            const double* __restrict__ a, StepArgs s)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.n) return;
-    double xn[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int e = 3 * i + k;
-        const double vi = v[e], ai = a[e];
-        xn[k] = drift1(x[e], vi, ai, s, k);
-        x[e] = xn[k];
-        vold[e] = vi;
-        v[e] = __dadd_rn(vi, __dmul_rn(s.dt, ai));
-    }
-    store_pos(pos, posf, iperm[i], xn, s.pack_w ? zii[i] : 0.0);
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * s.n) return;
+    const double xi = x[e], vi = v[e], ai = a[e];
+    x[e] = drift1(xi, vi, ai, s, e % 3);
+    vold[e] = vi;
+    v[e] = __dadd_rn(vi, __dmul_rn(s.dt, ai));
 }
 
-// VV1 first half: drift, v += dt/2 a (vel_verlet_1.f:148-166).
+// VV1 first half: drift, v += dt/2 a (vel_verlet_1.f:148-166); one thread
+// per element.
 static __global__ void k_drift_vv1(double* __restrict__ x, double* __restrict__ v,
-                            const double* __restrict__ a, const double* __restrict__ zii,
-                            const int* __restrict__ iperm, double4* __restrict__ pos,
-                            float* __restrict__ posf, StepArgs s)
+                            const double* __restrict__ a, StepArgs s)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.n) return;
-    double xn[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int e = 3 * i + k;
-        const double ai = a[e];
-        xn[k] = drift1(x[e], v[e], ai, s, k);
-        x[e] = xn[k];
-        v[e] = __dadd_rn(v[e], __dmul_rn(s.halfdt, ai));
-    }
-    store_pos(pos, posf, iperm[i], xn, s.pack_w ? zii[i] : 0.0);
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * s.n) return;
+    const double xi = x[e], vi = v[e], ai = a[e];
+    x[e] = drift1(xi, vi, ai, s, e % 3);
+    v[e] = __dadd_rn(vi, __dmul_rn(s.halfdt, ai));
 }
 
 // VV3 first half: drift and the first Spreiter-Walter stage
 // (vel_verlet_3.f:255-262; v(2,i) reads the already updated v(1,i)).
 static __global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ v,
                             const double* __restrict__ a, const double* __restrict__ zii,
-                            const double* __restrict__ aii, const int* __restrict__ iperm,
-                            double4* __restrict__ pos, float* __restrict__ posf, StepArgs s)
+                            const double* __restrict__ aii, StepArgs s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
-    double xn[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int e = 3 * i + k;
-        xn[k] = drift1(x[e], v[e], a[e], s, k);
-        x[e] = xn[k];
-    }
-    const double omega = __ddiv_rn(__dmul_rn(__dmul_rn(s.lorentz_c, zii[i]), s.bfield), aii[i]);
-    const double w = __dmul_rn(s.halfdt, omega);
-    const double w2 = __dmul_rn(w, w);
+    const double x1 = x[3 * i], x2 = x[3 * i + 1], x3 = x[3 * i + 2];
     const double a1 = a[3 * i], a2 = a[3 * i + 1], a3 = a[3 * i + 2];
     double v1 = v[3 * i], v2 = v[3 * i + 1], v3 = v[3 * i + 2];
+    const double zi = zii[i], ai = aii[i];
+    x[3 * i] = drift1(x1, v1, a1, s, 0);
+    x[3 * i + 1] = drift1(x2, v2, a2, s, 1);
+    x[3 * i + 2] = drift1(x3, v3, a3, s, 2);
+    const double omega = __ddiv_rn(__dmul_rn(__dmul_rn(s.lorentz_c, zi), s.bfield), ai);
+    const double w = __dmul_rn(s.halfdt, omega);
+    const double w2 = __dmul_rn(w, w);
     v1 = __dadd_rn(__dadd_rn(__dmul_rn(__dsub_rn(1.0, w2), v1), __dmul_rn(__dmul_rn(2.0, w), v2)),
                    __dmul_rn(s.halfdt, __dadd_rn(a1, __dmul_rn(w, a2))));
     v2 = __dadd_rn(__dsub_rn(__dmul_rn(__dsub_rn(1.0, w2), v2), __dmul_rn(__dmul_rn(2.0, w), v1)),
@@ -124,7 +124,6 @@ static __global__ void k_drift_vv3(double* __restrict__ x, double* __restrict__ 
     v[3 * i] = v1;
     v[3 * i + 1] = v2;
     v[3 * i + 2] = v3;
-    store_pos(pos, posf, iperm[i], xn, s.pack_w ? zii[i] : 0.0);
 }
 
 template <bool KIN>
@@ -167,9 +166,10 @@ k_post_vv2(double* __restrict__ v, const double* __restrict__ vold, double* __re
             a[3 * i] = aa[0];
             a[3 * i + 1] = aa[1];
         }
+        const double vo[3] = {vold[3 * i], vold[3 * i + 1], vold[3 * i + 2]};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const double vp = __dadd_rn(vold[3 * i + k], __dmul_rn(s.dt, aa[k]));
+            const double vp = __dadd_rn(vo[k], __dmul_rn(s.dt, aa[k]));
             vv[k] = __dmul_rn(0.5, __dadd_rn(vv[k], vp));
             v[3 * i + k] = vv[k];
         }
@@ -187,13 +187,19 @@ k_post_vv1(double* __restrict__ v, const double* __restrict__ a, const double* _
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double t[NKIN] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i < s.n) {
-        double vv[3];
+        double vv[3], aa[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            vv[k] = __dadd_rn(v[3 * i + k], __dmul_rn(s.halfdt, a[3 * i + k]));
+            vv[k] = v[3 * i + k];
+            aa[k] = a[3 * i + k];
+        }
+        const double am = aii[i];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            vv[k] = __dadd_rn(vv[k], __dmul_rn(s.halfdt, aa[k]));
             v[3 * i + k] = vv[k];
         }
-        kin_sums<true>(t, aii[i], vv[0], vv[1], vv[2]);
+        kin_sums<true>(t, am, vv[0], vv[1], vv[2]);
     }
     block_sum_store<NKIN>(t, red, kpart + (size_t)blockIdx.x * NKIN);
 }
