@@ -254,6 +254,8 @@ k_force_pairs_batch(const double4* __restrict__ pos, const float* __restrict__ p
         bx.posf = posf + (size_t)(d->S / SHADOW_TILE) * SHADOW_FLOATS;
         bx.Si = Si + d->Si_off;
         bx.Sj = Sj + d->Sj_off;
+        bx.tbox = nullptr;
+        bx.Sjf = nullptr;
         bx.n = sfa.n;
         bx.M = d->T;
         bx.nseg_max = d->nseg;

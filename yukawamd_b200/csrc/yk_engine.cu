@@ -154,6 +154,8 @@ struct yk_ctx {
     // half-pair kernel
     double *Si = nullptr, *Sm = nullptr;
     void* Sj = nullptr;                 // source-side rows: double (FP64 form) or float (mixed form)
+    float* tbox = nullptr;              // tile boxes (k_tile_boxes), 8 floats per tile
+    unsigned char* Sjf = nullptr;       // per unit: its Sj row was written
     int4* jobs = nullptr;
     int* row_slots = nullptr;
     int* job_counter = nullptr;
@@ -441,7 +443,8 @@ static size_t pair_scratch_bytes(int n, int seg, int dev, int precision)
     build_pair_jobs(M, seg, pair_ctas(dev), jobs, slots);
     const size_t nseg = M > 0 ? (size_t)*std::max_element(slots.begin(), slots.end()) : 0;
     return sj_bytes + sizeof(double) * ((size_t)M * nseg * PB * 3 + jobs.size() * NSCAL) +
-           sizeof(int4) * jobs.size() + sizeof(int) * (size_t)M;
+           sizeof(int4) * jobs.size() + sizeof(int) * (size_t)M + sizeof(float) * 8 * (size_t)M +
+           (size_t)M * (M + 1) / 2;
 }
 
 static void free_pairs(yk_ctx* c)
@@ -455,6 +458,10 @@ static void free_pairs(yk_ctx* c)
     c->jobs = nullptr;
     cudaFree(c->row_slots);
     c->row_slots = nullptr;
+    cudaFree(c->tbox);
+    c->tbox = nullptr;
+    cudaFree(c->Sjf);
+    c->Sjf = nullptr;
     c->pj = PairJobs{};
 }
 
@@ -477,6 +484,8 @@ static int setup_pairs(yk_ctx* c)
     CK(c, cudaMalloc((void**)&c->Sm, sizeof(double) * jobs.size() * NSCAL));
     CK(c, cudaMalloc((void**)&c->jobs, sizeof(int4) * jobs.size()));
     CK(c, cudaMalloc((void**)&c->row_slots, sizeof(int) * (size_t)std::max(M, 1)));
+    CK(c, cudaMalloc((void**)&c->tbox, sizeof(float) * 8 * (size_t)std::max(M, 1)));
+    CK(c, cudaMalloc((void**)&c->Sjf, std::max<size_t>(units, 1)));
     CK(c, cudaMemcpy(c->jobs, jobs.data(), sizeof(int4) * jobs.size(), cudaMemcpyHostToDevice));
     CK(c, cudaMemcpy(c->row_slots, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice));
     c->pj.jobs = c->jobs;
@@ -484,6 +493,8 @@ static int setup_pairs(yk_ctx* c)
     c->pj.njobs = (int)jobs.size();
     c->pj.M = M;
     c->pj.nseg_max = nseg;
+    c->pj.tbox = c->tbox;
+    c->pj.Sjf = c->Sjf;
     return YK_OK;
 }
 
@@ -585,30 +596,47 @@ static int launch_force_t(yk_ctx* c)
         return 1;
     }
     cudaMemsetAsync(c->job_counter, 0, sizeof(int), c->stream);
+    PairJobs pj = c->pj;
+    row_t<PREC>* Sj = static_cast<row_t<PREC>*>(c->Sj);
+    const int njobs = c->pj.njobs;
+    int k = 2;
     if (c->kernel == 3) {
+        // the near-list kernel writes every Sj row and takes no tile boxes
+        pj.tbox = nullptr;
+        pj.Sjf = nullptr;
         const int grid = persistent_grid<k_force_near<SIM, PREC, MEAS>>(c->dev);
-        k_force_near<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-            c->pos, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
-    } else if (lo_path<SIM, PREC>(c->fa)) {
-        if constexpr (PREC == PREC_MIXED) {
-            const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(c->dev);
-            k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
-        }
-    } else if (SIM != SIM_NUCLEON && c->fa.img_k) {
-        if constexpr (SIM != SIM_NUCLEON) {
-            const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, false, true>>(c->dev);
-            k_force_pairs<SIM, PREC, MEAS, false, true><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-                c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
-        }
+        k_force_near<SIM, PREC, MEAS><<<std::min(grid, njobs), PB, 0, c->stream>>>(
+            c->pos, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
     } else {
-        const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS>>(c->dev);
-        k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, c->pj.njobs), PB, 0, c->stream>>>(
-            c->pos, c->posf, c->pj, c->job_counter, c->fa, c->Si, static_cast<row_t<PREC>*>(c->Sj), c->Sm, c->err);
+        if (lo_path<SIM, PREC>(c->fa) && pairs_tile_boxes<SIM, PREC, true>()) {
+            k_tile_boxes<<<c->pj.M, PB, 0, c->stream>>>(c->posf, c->n, c->fa, c->tbox);
+            ++k;
+        } else {
+            pj.tbox = nullptr;
+        }
+        if (lo_path<SIM, PREC>(c->fa)) {
+            if constexpr (PREC == PREC_MIXED) {
+                const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, true>>(c->dev);
+                k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, njobs), PB, 0, c->stream>>>(
+                    c->pos, c->posf, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
+            }
+        } else if (SIM != SIM_NUCLEON && c->fa.img_k) {
+            if constexpr (SIM != SIM_NUCLEON) {
+                const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, false, true>>(c->dev);
+                k_force_pairs<SIM, PREC, MEAS, false, true><<<std::min(grid, njobs), PB, 0, c->stream>>>(
+                    c->pos, c->posf, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
+            }
+        } else {
+            const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS>>(c->dev);
+            k_force_pairs<SIM, PREC, MEAS><<<std::min(grid, njobs), PB, 0, c->stream>>>(
+                c->pos, c->posf, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
+        }
     }
-    k_combine<SIM, PREC><<<c->pj.M, COMB_THREADS, 0, c->stream>>>(c->Si, static_cast<row_t<PREC>*>(c->Sj), c->pj, c->perm, c->zii,
-                                                              c->aii, c->fa, c->a);
-    return 2;
+    // dynamic shared memory: the unit flags of one row (M bytes at most)
+    const size_t fl_bytes = pj.Sjf ? (size_t)c->pj.M : 0;
+    k_combine<SIM, PREC><<<c->pj.M, COMB_THREADS, fl_bytes, c->stream>>>(c->Si, Sj, pj, c->perm, c->zii, c->aii,
+                                                                         c->fa, c->a);
+    return k;
 }
 
 template <int SIM>

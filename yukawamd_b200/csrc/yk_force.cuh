@@ -719,11 +719,20 @@ template <bool MEAS>
 struct TargetAcc<PREC_MIXED, MEAS> {
     cf32 f[3];
     cf32 s[MEAS ? NSCAL : 1];
+    // FP64 sums of the group sums that add_group2 takes (the hi/lo pair paths):
+    // one conversion and one FP64 add per component on pipes the FP32 pair
+    // arithmetic leaves idle, instead of seven FP32 operations of a two-sum
+    double fd[3];
+    double sd[MEAS ? NSCAL : 1];
     __device__ __forceinline__ void zero()
     {
         f[0] = f[1] = f[2] = cf32();
+        fd[0] = fd[1] = fd[2] = 0.0;
 #pragma unroll
-        for (int k = 0; k < (MEAS ? NSCAL : 1); ++k) s[k] = cf32();
+        for (int k = 0; k < (MEAS ? NSCAL : 1); ++k) {
+            s[k] = cf32();
+            sd[k] = 0.0;
+        }
     }
     __device__ __forceinline__ void add(const PairOut<float>& o, float weight)
     {
@@ -754,20 +763,21 @@ struct TargetAcc<PREC_MIXED, MEAS> {
             for (int k = 0; k < NSCAL; ++k) s[k].add(g.s[k]);
         }
     }
-    // add_group with the compensated sums advanced two at a time
+    // a group's plain FP32 sum into the FP64 sums (exact conversion, one
+    // FP64 rounding per group)
     __device__ __forceinline__ void add_group2(const GroupSum<PREC_MIXED, MEAS>& g)
     {
-        cf32_add2(f[0], f[1], make_float2(g.f[0], g.f[1]));
-        f[2].add(g.f[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fd[c] += (double)g.f[c];
         if constexpr (MEAS) {
 #pragma unroll
-            for (int k = 0; k < NSCAL; k += 2) cf32_add2(s[k], s[k + 1], make_float2(g.s[k], g.s[k + 1]));
+            for (int k = 0; k < NSCAL; ++k) sd[k] += (double)g.s[k];
         }
     }
-    __device__ __forceinline__ double force(int k) const { return f[k].value(); }
+    __device__ __forceinline__ double force(int k) const { return f[k].value() + fd[k]; }
     __device__ __forceinline__ double scal(int k) const
     {
-        if constexpr (MEAS) return s[k].value();
+        if constexpr (MEAS) return s[k].value() + sd[k];
         return 0.0;
     }
 };

@@ -278,6 +278,8 @@ k_force_near(const double4* __restrict__ pos, PairJobs pj, int* __restrict__ job
     bx.posf = nullptr;
     bx.Si = Si;
     bx.Sj = Sj;
+    bx.tbox = nullptr;
+    bx.Sjf = nullptr;
     bx.n = fa.n;
     bx.M = pj.M;
     bx.nseg_max = pj.nseg_max;

@@ -62,7 +62,57 @@ struct PairJobs {
     int njobs;
     int M;                        // tiles
     int nseg_max;                 // Si slots per row in the layout (max of row_slots)
+    // optional (null: every warp screens every tile, every Sj row is written):
+    const float* tbox;            // per tile: centre[3], pad, half-width[3], pad (k_tile_boxes)
+    unsigned char* Sjf;           // per unit tri(C,R): 1 if its Sj row was written,
+                                  // 0 if the row is zero and was not written
 };
+
+// Bounding box of each 128-slot tile on the FP32 shadow hi parts (the
+// coordinates near_groups screens), with the warp box's rounding margin:
+// one CTA of PB threads per tile.
+static __global__ void __launch_bounds__(PB)
+k_tile_boxes(const float* __restrict__ posf, int n, ForceArgs fa, float* __restrict__ tbox)
+{
+    __shared__ float red[PWARPS][6];
+    const int C = blockIdx.x, j = threadIdx.x, lane = j & 31, warp = j >> 5;
+    const float inf = __int_as_float(0x7f800000);
+    const bool on = C * PB + j < n;
+    const float* t = posf + (size_t)C * SHADOW_FLOATS;
+    float lo[3], hi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float v = t[shadow_off(j, k)];
+        float a = on ? v : inf, b = on ? v : -inf;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a = fminf(a, __shfl_xor_sync(0xffffffffu, a, o));
+            b = fmaxf(b, __shfl_xor_sync(0xffffffffu, b, o));
+        }
+        lo[k] = a;
+        hi[k] = b;
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            red[warp][k] = lo[k];
+            red[warp][3 + k] = hi[k];
+        }
+    __syncthreads();
+    if (j < 3) {
+        float a = red[0][j], b = red[0][3 + j];
+#pragma unroll
+        for (int w = 1; w < PWARPS; ++w) {
+            a = fminf(a, red[w][j]);
+            b = fmaxf(b, red[w][3 + j]);
+        }
+        const float mu = fmaf(3.814697265625e-6f, fa.Lf[j], (float)(2.0 * SHADOW_Q));
+        tbox[8 * C + j] = 0.5f * (a + b);
+        tbox[8 * C + 4 + j] = fmaf(0.5f, b - a, mu);
+    } else if (j == 3 || j == 7) {
+        tbox[8 * C + j] = 0.f;
+    }
+}
 
 __host__ __device__ __forceinline__ long long tri_index(int C, int R)
 {
@@ -546,6 +596,33 @@ __device__ __forceinline__ bool box_reaches(const ForceArgs& fa, const WarpBox& 
     return dist2 <= lim;
 }
 
+// Whether any source of a tile can reach the warp's box: the box_reaches
+// bound with the tile's box in place of the source.  Per axis the minimum-
+// image distance is a metric, so a source within the tile's half-width tb[4+k]
+// of its centre tb[k] is at least |mi(tb[k] - c)| - tb[4+k] from the warp
+// centre: if the boxes are out of reach, so is every source of the tile.
+// (Nucleons: the Coulomb radius counts if the warp has a proton target.)
+template <int SIM>
+__device__ __forceinline__ bool tile_reaches(const ForceArgs& fa, const WarpBox& b, const float* tb)
+{
+    const float MAGIC = 12582912.0f;
+    float dist2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float d = tb[k] - b.c[k];
+        const float dm = fmaf(-fa.Lf[k], fmaf(d, fa.invLf[k], MAGIC) - MAGIC, d);
+        const float m = fmaxf(fabsf(dm) - b.h[k] - tb[4 + k], 0.f);
+        dist2 = fmaf(m, m, dist2);
+    }
+    float lim;
+    if constexpr (SIM == SIM_PURE || SIM == SIM_MIX) {
+        lim = fa.scr_c2;
+    } else {
+        lim = (b.has_p && fa.coulomb_on) ? fmaxf(fa.scr_c2, fa.scr_n2) : fa.scr_n2;
+    }
+    return dist2 <= lim;
+}
+
 // Bits 4k..4k+3 of v -> bit k (k = 0..7): which of 8 groups has a set bit.
 __device__ __forceinline__ unsigned any_of_4(unsigned v)
 {
@@ -640,10 +717,12 @@ template <typename RowT>
 struct PairSmem {
     double4 tile[2][PB];                  // FP64 source tiles, or the shadow lo parts (TMA)
     float tilef[2][SHADOW_HI_FLOATS];     // FP32 shadow source tiles, hi parts and w (TMA)
+    alignas(16) float tb[2][8];           // the tiles' boxes (TMA, when PairJobs::tbox is set)
     RowT acc_j[2][PWARPS][PB * 3];        // per-warp reaction rows, one set per tile stage
     double red[32 * NSCAL];               // block reduction scratch
     uint64_t bar[2];                      // one mbarrier per tile stage
     int done[2];                          // warps finished with the stage's tile
+    int used[2][PWARPS];                  // the warp wrote its row of the stage's tile
     int abort;                            // a tile copy timed out: every warp leaves
     int s_job;
 };
@@ -655,6 +734,8 @@ struct BoxView {
     const float* posf;
     double* Si;
     void* Sj;                      // source-side rows, row_t of the form
+    const float* tbox;             // tile boxes, or null (PairJobs::tbox)
+    unsigned char* Sjf;            // Sj row flags, or null (PairJobs::Sjf)
     int n, M, nseg_max;
 };
 
@@ -680,9 +761,11 @@ __device__ __forceinline__ void pairs_smem_init(PairSmem<RowT>& sm)
 static_assert(SHADOW_LO_FLOATS * sizeof(float) <= PB * sizeof(double4), "lo parts must fit a tile stage");
 
 // Load source tile C of box bx into stage qq & 1 (one thread): the shadow hi
-// parts, and the FP64 positions or (lo) the shadow lo parts.
+// parts, the FP64 positions or (lo) the shadow lo parts, and (tb) the tile's
+// box.
 template <typename RowT>
-__device__ __forceinline__ void pairs_issue(PairSmem<RowT>& sm, const BoxView& bx, int C, unsigned qq, bool lo)
+__device__ __forceinline__ void pairs_issue(PairSmem<RowT>& sm, const BoxView& bx, int C, unsigned qq, bool lo,
+                                            bool tb)
 {
     const int j0 = C * PB;
     const int cnt = min(PB, bx.n - j0);
@@ -691,10 +774,12 @@ __device__ __forceinline__ void pairs_issue(PairSmem<RowT>& sm, const BoxView& b
     const unsigned bytesf = (unsigned)SHADOW_HI_FLOATS * (unsigned)sizeof(float);
     const float* src = bx.posf + (size_t)C * SHADOW_FLOATS;
     uint64_t* b = &sm.bar[qq & 1];
-    mbar_arrive_expect_tx(b, bytes + bytesf);
+    const unsigned bytesb = (tb && bx.tbox) ? 8u * (unsigned)sizeof(float) : 0u;
+    mbar_arrive_expect_tx(b, bytes + bytesf + bytesb);
     if (lo) bulk_g2s(&sm.tile[qq & 1][0], src + SHADOW_HI_FLOATS, bytes, b);
     else bulk_g2s(&sm.tile[qq & 1][0], bx.pos + j0, bytes, b);
     bulk_g2s(&sm.tilef[qq & 1][0], src, bytesf, b);
+    if (bytesb) bulk_g2s(&sm.tb[qq & 1][0], bx.tbox + 8 * (size_t)C, bytesb, b);
 }
 
 // Job (R, sg) of box bx: target block R against source tiles
@@ -715,7 +800,7 @@ __device__ __forceinline__ void pairs_issue(PairSmem<RowT>& sm, const BoxView& b
 // hi/lo parts (pair_group_lo): 0 never, 1 always (the caller has checked
 // fa.lo; the FP64-tile path is then not compiled in, which frees its
 // registers), 2 as fa.lo says (boxes of a batch differ).
-template <int SIM, int PREC, bool MEAS, int LOMODE = 2, bool IMGK = false>
+template <int SIM, int PREC, bool MEAS, int LOMODE = 2, bool IMGK = false, bool TB = false>
 __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const ForceArgs& fa, const BoxView& bx, int R,
                                           int C0, int C1, int sg, double* __restrict__ sm_row,
                                           unsigned* __restrict__ err, unsigned& q)
@@ -750,12 +835,13 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
 #pragma unroll
         for (int c = 0; c < 3; ++c) nli[c] = -bx.posf[shadow_index(active ? i : 0, 4 + c)];
     }
+    const bool tb = TB && bx.tbox != nullptr;
 
     // both stages are free: every warp has passed the block barrier that
     // handed out this job
     if (tid == 0) {
-        pairs_issue(sm, bx, C0, q, lo);
-        if (C0 + 1 < C1) pairs_issue(sm, bx, C0 + 1, q + 1, lo);
+        pairs_issue(sm, bx, C0, q, lo, tb);
+        if (C0 + 1 < C1) pairs_issue(sm, bx, C0 + 1, q + 1, lo, tb);
     }
     const unsigned q0 = q;
     for (int C = C0; C < C1; ++C, ++q) {
@@ -766,119 +852,137 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
         const double4* tl = sm.tile[st];
         const float* tlf = sm.tilef[st];
         row_t<PREC>* my_acc = sm.acc_j[st][warp];
+        // The warp's row is used (zeroed, then written group by group) only
+        // if some group of the tile is near its targets; otherwise it is
+        // marked unused.  TB: a tile whose box is out of reach of the warp's
+        // box is skipped before the per-source screen.
+        bool used = false;
+        auto open_row = [&](unsigned gm) {
+            used = gm != 0;
+            if (used) {
 #pragma unroll
-        for (int k = lane; k < PB * 3; k += 32) my_acc[k] = 0.0;
-        __syncwarp();
-        // on the diagonal tile only sources after the warp's first target count
-        const int jmin = max(diag ? 32 * warp + 1 : 0, w0);
-        const bool full = !diag && jlim == PB && all_active && w0 == 0;
-        if (lo) {
-            if constexpr (PREC == PREC_MIXED && SIM == SIM_NUCLEON) {
+                for (int k = lane; k < PB * 3; k += 32) my_acc[k] = 0.0;
+                __syncwarp();
+            }
+        };
+        const bool reach = box.any && (!tb || tile_reaches<SIM>(fa, box, sm.tb[st]));
+        if (reach) {
+            // on the diagonal tile only sources after the warp's first target count
+            const int jmin = max(diag ? 32 * warp + 1 : 0, w0);
+            const bool full = !diag && jlim == PB && all_active && w0 == 0;
+            if (lo) {
+                if constexpr (PREC == PREC_MIXED && SIM == SIM_NUCLEON) {
+                    unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
+                    open_row(gm);
+                    const float* tll = reinterpret_cast<const float*>(tl);
+                    const double4* gsrc = bx.pos + (size_t)C * PB;
+                    if (full) {
+                        for (; gm; gm &= gm - 1)
+                            pair_group_nn_lo<MEAS, false>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
+                                                          diag, active, tid, sw, acc, my_acc);
+                    } else {
+                        for (; gm; gm &= gm - 1)
+                            pair_group_nn_lo<MEAS, true>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
+                                                         diag, active, tid, sw, acc, my_acc);
+                    }
+                }
+                if constexpr (PREC == PREC_MIXED && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+                    int kcode = -1;
+                    unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
+                    open_row(gm);
+                    const float* tll = reinterpret_cast<const float*>(tl);
+                    if (box.tile_img && kcode >= 0) {
+                        // one image for the whole tile: fold it into the target
+                        float2 th[3], tl2[3];
+                        const float nh[3] = {si.nx, si.ny, si.nz};
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const float k = img_of(kcode, c);
+                            const float h = fmaf(-k, fa.Lh[c], nh[c]);       // exact
+                            const float l = fmaf(-k, fa.Ll[c], nli[c]);
+                            th[c] = make_float2(h, h);
+                            tl2[c] = make_float2(l, l);
+                        }
+                        if (full) {
+                            for (; gm; gm &= gm - 1)
+                                pair_group_lo<SIM, MEAS, false, true>(fa, si, nli, th, tl2, wi, tlf, tll,
+                                                                      4 * (__ffs(gm) - 1), jlim, diag, active, tid,
+                                                                      sw, acc, my_acc);
+                        } else {
+                            for (; gm; gm &= gm - 1)
+                                pair_group_lo<SIM, MEAS, true, true>(fa, si, nli, th, tl2, wi, tlf, tll,
+                                                                     4 * (__ffs(gm) - 1), jlim, diag, active, tid,
+                                                                     sw, acc, my_acc);
+                        }
+                    } else {
+                        const float2 z[3] = {};
+                        if (full) {
+                            for (; gm; gm &= gm - 1)
+                                pair_group_lo<SIM, MEAS, false>(fa, si, nli, z, z, wi, tlf, tll, 4 * (__ffs(gm) - 1),
+                                                                jlim, diag, active, tid, sw, acc, my_acc);
+                        } else {
+                            for (; gm; gm &= gm - 1)
+                                pair_group_lo<SIM, MEAS, true>(fa, si, nli, z, z, wi, tlf, tll, 4 * (__ffs(gm) - 1),
+                                                               jlim, diag, active, tid, sw, acc, my_acc);
+                        }
+                    }
+                }
+            } else if (IMGK && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+                // ions whose screen image integers are exact: the tile image
+                // when the tile has one, else each pair's own
+                if constexpr (IMGK && (SIM == SIM_PURE || SIM == SIM_MIX)) {
+                    int kcode = -1;
+                    unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
+                    open_row(gm);
+                    if (box.tile_img && kcode >= 0) {
+                        float2 th[3];
+                        const float nh[3] = {si.nx, si.ny, si.nz};
+                        const double pc[3] = {pi.x, pi.y, pi.z};
+                        double pt[3];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const float k = img_of(kcode, c);
+                            const float h = fmaf(-k, fa.Lh[c], nh[c]);       // exact
+                            th[c] = make_float2(h, h);
+                            pt[c] = __fma_rn((double)k, fa.xl[c], pc[c]);
+                        }
+                        const double4 pit = make_double4(pt[0], pt[1], pt[2], pi.w);
+                        if (full) {
+                            for (; gm; gm &= gm - 1)
+                                pair_group<SIM, PREC, MEAS, false, true, true>(fa, pi, si, wi, tl, tlf,
+                                                                               4 * (__ffs(gm) - 1), jlim, diag, active,
+                                                                               tid, sw, acc, my_acc, th, pit);
+                        } else {
+                            for (; gm; gm &= gm - 1)
+                                pair_group<SIM, PREC, MEAS, true, true, true>(fa, pi, si, wi, tl, tlf,
+                                                                              4 * (__ffs(gm) - 1), jlim, diag, active,
+                                                                              tid, sw, acc, my_acc, th, pit);
+                        }
+                    } else if (full) {
+                        for (; gm; gm &= gm - 1)
+                            pair_group<SIM, PREC, MEAS, false, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                                                                     diag, active, tid, sw, acc, my_acc);
+                    } else {
+                        for (; gm; gm &= gm - 1)
+                            pair_group<SIM, PREC, MEAS, true, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                                                                    diag, active, tid, sw, acc, my_acc);
+                    }
+                }
+            } else {
                 unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
-                const float* tll = reinterpret_cast<const float*>(tl);
-                const double4* gsrc = bx.pos + (size_t)C * PB;
+                open_row(gm);
                 if (full) {
                     for (; gm; gm &= gm - 1)
-                        pair_group_nn_lo<MEAS, false>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
-                                                      diag, active, tid, sw, acc, my_acc);
-                } else {
-                    for (; gm; gm &= gm - 1)
-                        pair_group_nn_lo<MEAS, true>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
-                                                     diag, active, tid, sw, acc, my_acc);
-                }
-            }
-            if constexpr (PREC == PREC_MIXED && (SIM == SIM_PURE || SIM == SIM_MIX)) {
-                int kcode = -1;
-                unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
-                const float* tll = reinterpret_cast<const float*>(tl);
-                if (box.tile_img && kcode >= 0) {
-                    // one image for the whole tile: fold it into the target
-                    float2 th[3], tl2[3];
-                    const float nh[3] = {si.nx, si.ny, si.nz};
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const float k = img_of(kcode, c);
-                        const float h = fmaf(-k, fa.Lh[c], nh[c]);       // exact
-                        const float l = fmaf(-k, fa.Ll[c], nli[c]);
-                        th[c] = make_float2(h, h);
-                        tl2[c] = make_float2(l, l);
-                    }
-                    if (full) {
-                        for (; gm; gm &= gm - 1)
-                            pair_group_lo<SIM, MEAS, false, true>(fa, si, nli, th, tl2, wi, tlf, tll,
-                                                                  4 * (__ffs(gm) - 1), jlim, diag, active, tid,
-                                                                  sw, acc, my_acc);
-                    } else {
-                        for (; gm; gm &= gm - 1)
-                            pair_group_lo<SIM, MEAS, true, true>(fa, si, nli, th, tl2, wi, tlf, tll,
-                                                                 4 * (__ffs(gm) - 1), jlim, diag, active, tid,
-                                                                 sw, acc, my_acc);
-                    }
-                } else {
-                    const float2 z[3] = {};
-                    if (full) {
-                        for (; gm; gm &= gm - 1)
-                            pair_group_lo<SIM, MEAS, false>(fa, si, nli, z, z, wi, tlf, tll, 4 * (__ffs(gm) - 1),
-                                                            jlim, diag, active, tid, sw, acc, my_acc);
-                    } else {
-                        for (; gm; gm &= gm - 1)
-                            pair_group_lo<SIM, MEAS, true>(fa, si, nli, z, z, wi, tlf, tll, 4 * (__ffs(gm) - 1),
-                                                           jlim, diag, active, tid, sw, acc, my_acc);
-                    }
-                }
-            }
-        } else if (IMGK && (SIM == SIM_PURE || SIM == SIM_MIX)) {
-            // ions whose screen image integers are exact: the tile image
-            // when the tile has one, else each pair's own
-            if constexpr (IMGK && (SIM == SIM_PURE || SIM == SIM_MIX)) {
-                int kcode = -1;
-                unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
-                if (box.tile_img && kcode >= 0) {
-                    float2 th[3];
-                    const float nh[3] = {si.nx, si.ny, si.nz};
-                    const double pc[3] = {pi.x, pi.y, pi.z};
-                    double pt[3];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const float k = img_of(kcode, c);
-                        const float h = fmaf(-k, fa.Lh[c], nh[c]);       // exact
-                        th[c] = make_float2(h, h);
-                        pt[c] = __fma_rn((double)k, fa.xl[c], pc[c]);
-                    }
-                    const double4 pit = make_double4(pt[0], pt[1], pt[2], pi.w);
-                    if (full) {
-                        for (; gm; gm &= gm - 1)
-                            pair_group<SIM, PREC, MEAS, false, true, true>(fa, pi, si, wi, tl, tlf,
-                                                                           4 * (__ffs(gm) - 1), jlim, diag, active,
-                                                                           tid, sw, acc, my_acc, th, pit);
-                    } else {
-                        for (; gm; gm &= gm - 1)
-                            pair_group<SIM, PREC, MEAS, true, true, true>(fa, pi, si, wi, tl, tlf,
-                                                                          4 * (__ffs(gm) - 1), jlim, diag, active,
-                                                                          tid, sw, acc, my_acc, th, pit);
-                    }
-                } else if (full) {
-                    for (; gm; gm &= gm - 1)
-                        pair_group<SIM, PREC, MEAS, false, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                        pair_group<SIM, PREC, MEAS, false, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
                                                                  diag, active, tid, sw, acc, my_acc);
                 } else {
                     for (; gm; gm &= gm - 1)
-                        pair_group<SIM, PREC, MEAS, true, true>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
+                        pair_group<SIM, PREC, MEAS, true, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
                                                                 diag, active, tid, sw, acc, my_acc);
                 }
             }
-        } else {
-            unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
-            if (full) {
-                for (; gm; gm &= gm - 1)
-                    pair_group<SIM, PREC, MEAS, false, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
-                                                             diag, active, tid, sw, acc, my_acc);
-            } else {
-                for (; gm; gm &= gm - 1)
-                    pair_group<SIM, PREC, MEAS, true, IMGK>(fa, pi, si, wi, tl, tlf, 4 * (__ffs(gm) - 1), jlim,
-                                                            diag, active, tid, sw, acc, my_acc);
-            }
         }
+        if (lane == 0) sm.used[st][warp] = used ? 1 : 0;
         // this warp is done with the tile: the last warp reduces and refills
         __threadfence_block();
         __syncwarp();
@@ -888,20 +992,32 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
         if (last) {
             __threadfence_block();
             if (lane == 0) sm.done[st] = 0;
-            // the unit's source-side row: FP64 in the FP64 form, FP32 (one
-            // rounding of the four warps' FP32 rows summed in FP64) in the
-            // mixed form
-            row_t<PREC>* dj = static_cast<row_t<PREC>*>(bx.Sj) + (size_t)tri_index(C, R) * PB * 3;
-            // (only this job's window: the other parts of a split unit write the rest)
-#pragma unroll 4
-            for (int k = 3 * w0 + lane; k < 3 * w1; k += 32) {
-                double v = sm.acc_j[st][0][k];
+            unsigned um = 0;
 #pragma unroll
-                for (int w = 1; w < PWARPS; ++w) v += sm.acc_j[st][w][k];
-                dj[k] = (row_t<PREC>)v;
+            for (int w = 0; w < PWARPS; ++w) um |= (unsigned)sm.used[st][w] << w;
+            const long long u = tri_index(C, R);
+            if (um == 0 && bx.Sjf && w0 == 0 && w1 == PB) {
+                // no warp had a pair: the unit's row is zero; k_combine skips it
+                if (lane == 0) bx.Sjf[u] = 0;
+            } else {
+                // the unit's source-side row: the used warp rows in warp order
+                // (an unused row is zero), FP64 in the FP64 form, FP32 (one
+                // rounding of the FP32 rows summed in FP64) in the mixed form;
+                // only this job's window (the other parts of a split unit
+                // write the rest)
+                row_t<PREC>* dj = static_cast<row_t<PREC>*>(bx.Sj) + (size_t)u * PB * 3;
+#pragma unroll 4
+                for (int k = 3 * w0 + lane; k < 3 * w1; k += 32) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int w = 0; w < PWARPS; ++w)
+                        if ((um >> w) & 1u) v += sm.acc_j[st][w][k];
+                    dj[k] = (row_t<PREC>)v;
+                }
+                if (lane == 0 && bx.Sjf) bx.Sjf[u] = 1;
             }
             __syncwarp();
-            if (lane == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2, lo);
+            if (lane == 0 && C + 2 < C1) pairs_issue(sm, bx, C + 2, q + 2, lo, tb);
         }
     }
     q = q0 + (unsigned)(C1 - C0);
@@ -933,6 +1049,17 @@ constexpr int pairs_ctas_per_sm()
     return (PREC == PREC_MIXED && LO) ? ((SIM == SIM_NUCLEON && !MEAS) ? 7 : 6) : 5;
 }
 
+// Whether a kernel variant tests each tile's box against each warp's box
+// (PairJobs::tbox) before screening its sources: the mixed hi/lo ion kernels,
+// whose per-group cost is low enough that the per-tile screen of far tiles
+// matters (9 % fewer instructions on the 55,296-ion mixture).  The FP64 and
+// nucleon kernels were slower with the test (register pressure).
+template <int SIM, int PREC, bool LO>
+constexpr bool pairs_tile_boxes()
+{
+    return PREC == PREC_MIXED && LO && SIM != SIM_NUCLEON;
+}
+
 // LO: the mixed ion kernel for boxes with fa.lo (pair_group_lo); IMGK: a
 // kernel for ion boxes with fa.img_k (the screen's image integers replace the
 // exact minimum-image comparisons, which are then not compiled in).
@@ -949,6 +1076,8 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
     bx.posf = posf;
     bx.Si = Si;
     bx.Sj = Sj;
+    bx.tbox = pj.tbox;
+    bx.Sjf = pj.Sjf;
     bx.n = fa.n;
     bx.M = pj.M;
     bx.nseg_max = pj.nseg_max;
@@ -959,8 +1088,9 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
         const int job = sm.s_job;
         if (job >= pj.njobs) break;
         const int4 js = pj.jobs[job];
-        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 0, IMGK>(sm, fa, bx, js.x, js.y, js.z, js.w,
-                                                          Sm + (size_t)job * NSCAL, err, q))
+        constexpr bool TB = pairs_tile_boxes<SIM, PREC, LO>();
+        if (!pairs_job<SIM, PREC, MEAS, LO ? 1 : 0, IMGK, TB>(sm, fa, bx, js.x, js.y, js.z, js.w,
+                                                              Sm + (size_t)job * NSCAL, err, q))
             return;
     }
 }
@@ -984,6 +1114,7 @@ k_combine(const double* __restrict__ Si, const row_t<PREC>* __restrict__ Sj, Pai
           const double* __restrict__ aii, ForceArgs fa, double* __restrict__ a_out)
 {
     __shared__ double part[COMB_GROUPS][PB * 3];
+    extern __shared__ unsigned char sfl[];      // row R's unit flags (pj.Sjf), R + 1 bytes
     const int R = pj.M - 1 - (int)blockIdx.x;
     const int g = threadIdx.x / (PB * 3), t = threadIdx.x % (PB * 3);
     constexpr size_t ROW = (size_t)PB * 3;
@@ -993,8 +1124,20 @@ k_combine(const double* __restrict__ Si, const row_t<PREC>* __restrict__ Sj, Pai
 #pragma unroll 4
     for (int s = g; s < nseg; s += COMB_GROUPS) F += si[(size_t)s * ROW];
     const row_t<PREC>* sj = Sj + (size_t)tri_index(R, 0) * ROW + t;
+    if (pj.Sjf) {
+        // rows flagged zero were not written (k_force_pairs); skipping them
+        // leaves every sum as it was.  The flags are staged in shared memory
+        // first, so that the row loads of the unrolled loop issue together.
+        const unsigned char* fl = pj.Sjf + tri_index(R, 0);
+        for (int r = threadIdx.x; r <= R; r += blockDim.x) sfl[r] = fl[r];
+        __syncthreads();
 #pragma unroll 4
-    for (int R2 = g; R2 <= R; R2 += COMB_GROUPS) F += (double)sj[(size_t)R2 * ROW];
+        for (int R2 = g; R2 <= R; R2 += COMB_GROUPS)
+            if (sfl[R2]) F += (double)sj[(size_t)R2 * ROW];
+    } else {
+#pragma unroll 4
+        for (int R2 = g; R2 <= R; R2 += COMB_GROUPS) F += (double)sj[(size_t)R2 * ROW];
+    }
     part[g][t] = F;
     __syncthreads();
     const int l = threadIdx.x;
