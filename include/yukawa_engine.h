@@ -314,6 +314,13 @@ typedef struct yk_tuning {
                              so split x more CTAs (threads per target) work on
                              a small box: 1, 2 or 4 (jobs of one tile then);
                              0 = 1; ignored by kernels 1 and 3.  Batches: 0/1 */
+    int targets_per_thread; /* targets each thread of the half-pair kernel
+                             holds: 1, or 2 (blocks of 256 targets, every
+                             source read and reaction reduction shared by two
+                             pairs) for ion boxes on the FP64 path with exact
+                             screen images or the mixed hi/lo path (other
+                             boxes take 1); 0 = automatic.  yk_get_tuning
+                             reports the value in use.  Batches: 0/1        */
 } yk_tuning;
 
 YK_API int yk_get_tuning(yk_ctx* ctx, yk_tuning* out);
@@ -361,6 +368,14 @@ YK_API int yk_peak_probe(int device, int kind, double* tflops);
  * Host arithmetic only (no GPU), for inspecting and testing the schedule.
  * No counterpart in the reference. */
 YK_API long long yk_pair_jobs(int m, int cap, int ctas, int* jobs, long long max_jobs, int* row_slots);
+
+/* The job table of the half-pair kernel with two targets per thread
+ * (yk_tuning.targets_per_thread = 2), same arguments: a job (R, C0, C1, slot)
+ * has R even and takes blocks R and R + 1 against source tiles C0 <= C < C1
+ * (C0 >= R), writing that slot of both rows' target-side partials; row_slots
+ * of both rows count the pair's jobs.  Host arithmetic only.  No counterpart
+ * in the reference. */
+YK_API long long yk_pair_jobs2(int m, int cap, int ctas, int* jobs, long long max_jobs, int* row_slots);
 
 /*
  * Force call that allocates no device memory.  No counterpart in the

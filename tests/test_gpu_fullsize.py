@@ -66,12 +66,18 @@ def nuc_ref(orc):
     return w, a, s
 
 
+@pytest.mark.parametrize("tpt", [1, 2], ids=["tpt1", "tpt2"])
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
-def test_ion_mixture_55296_every_particle(gpu, mix_ref, prec):
+def test_ion_mixture_55296_every_particle(gpu, mix_ref, prec, tpt):
     w, a_ref, s_ref = mix_ref
     with Engine(w.yk_params(precision=prec, mix_mode=abi.YK_MIX_COMPAT), w.x, w.v, w.zii, w.aii) as e:
+        assert e.set_tuning(targets_per_thread=tpt).targets_per_thread == tpt
         s = e.accel(True)
         _check(e.a, s, a_ref, s_ref, w.n, prec)
+        # force-only call after the measuring one: same forces within the tolerance
+        e.accel(False)
+        ft = _tols(prec)[0]
+        assert rel_norm(e.a[:3 * w.n], a_ref[:3 * w.n]) <= ft
 
 
 def _rows_nearest_half_box(w, count):

@@ -70,10 +70,11 @@ KERNELS = {"rows": dict(force_kernel=abi.KERNEL_ROWS),
            "near": dict(force_kernel=abi.KERNEL_NEAR),
            "near-unsorted-seg3": dict(force_kernel=abi.KERNEL_NEAR, sort_every=-1, pair_seg=3),
            "pairs-split2": dict(force_kernel=abi.KERNEL_PAIRS, source_split=2),
-           "pairs-split4-unsorted": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, source_split=4)}
+           "pairs-split4-unsorted": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, source_split=4),
+           "pairs-tpt2": dict(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=2)}
 
 
-@pytest.mark.parametrize("kern", list(KERNELS))
+@pytest.mark.parametrize("kern", [k for k in KERNELS if "tpt2" not in k])
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
 @pytest.mark.parametrize("meas", [True, False], ids=["meas", "force"])
 @pytest.mark.parametrize("kind,n", [("pure", 4096), ("mix", 3000), ("nn", 3000)])
@@ -171,7 +172,7 @@ def test_newton_steps_match_oracle(gpu, orc, kind):
     assert rel(s.px, s_ref.px) <= 1e-11
 
 
-@pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
+@pytest.mark.parametrize("kern", ["rows", "pairs", "near", "pairs-tpt2"])
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
 def test_run_graph_equals_newton_loop(gpu, prec, kern):
     """yk_run (CUDA graphs, Morton re-sorts inside) is bit-identical to the
@@ -241,6 +242,85 @@ def test_state_round_trip_and_box(gpu, orc):
         assert rel(s.ev, s_ref.ev) <= FP64_TOL
 
 
+def _short_cutoff(w, frac):
+    """The workload with r_c = frac * L (below L/2, so that the screen's
+    image integers are exact and the two-target kernel applies)."""
+    import copy
+    w2 = copy.deepcopy(w)
+    w2.params["rccut"] = frac * min(w.params["xl"])
+    return w2
+
+
+TPT2 = {"tpt2": dict(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=2),
+        "tpt2-unsorted-seg3": dict(force_kernel=abi.KERNEL_PAIRS, sort_every=-1, pair_seg=3, targets_per_thread=2),
+        "tpt2-seg1": dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, targets_per_thread=2)}
+
+
+def check_tpt2(orc, w, prec, meas, kern, mix_mode=abi.YK_MIX_COMPAT):
+    """check_accel on the two-target kernel, asserting that it ran."""
+    p = w.yk_params(precision=prec, mix_mode=mix_mode)
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        assert e.set_tuning(**TPT2[kern]).targets_per_thread == 2
+    check_accel(orc, w, prec, meas, mix_mode=mix_mode, tuning=TPT2[kern])
+
+
+@pytest.mark.parametrize("kern", list(TPT2))
+@pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("meas", [True, False], ids=["meas", "force"])
+@pytest.mark.parametrize("kind,n", [("pure", 4096), ("mix", 3000), ("mix", 6001)])
+def test_two_targets_per_thread_matches_oracle(gpu, orc, kind, n, meas, prec, kern):
+    """The two-target kernel (blocks of 256 targets) against the oracle: odd
+    and even tile counts, jobs cut to one and three tiles, unsorted slots."""
+    check_tpt2(orc, _short_cutoff(workload(kind, n, 300 + n), 0.4), prec, meas, kern)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 127, 128, 129, 255, 256, 257, 383, 385, 513])
+@pytest.mark.parametrize("kind", ["pure", "mix"])
+def test_two_targets_per_thread_ragged(gpu, orc, kind, n):
+    """Ragged sizes, including a last block pair with one block (odd tile
+    count) and partial tiles, FP64 and mixed, measuring and force-only."""
+    w = _short_cutoff(workload(kind, n, 11 + n), 0.35)
+    for prec in (abi.YK_PREC_FP64, abi.YK_PREC_MIXED):
+        check_tpt2(orc, w, prec, True, "tpt2")
+        check_tpt2(orc, w, prec, False, "tpt2-seg1")
+
+
+@pytest.mark.parametrize("mode", [abi.YK_MIX_COMPAT, abi.YK_MIX_FIXED], ids=["compat", "fixed"])
+def test_two_targets_per_thread_mix_modes(gpu, orc, mode):
+    w = _short_cutoff(workload("mix", 513, 5), 0.4)
+    check_tpt2(orc, w, abi.YK_PREC_FP64, True, "tpt2", mix_mode=mode)
+
+
+@pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
+def test_two_targets_per_thread_follows_the_box(gpu, orc, prec):
+    """targets_per_thread = 2 runs on ion boxes whose screen images are exact;
+    a box change that breaks that condition (the cutoff beyond L/2) takes the
+    one-target kernel, and a change back returns to two; the forces match the
+    oracle throughout.  Nucleon boxes always report 1."""
+    w = _short_cutoff(configs.ion_mixture_cfg(81, 3000), 0.4)
+    p = w.yk_params(precision=prec)
+    L = list(p.xl)
+    with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+        assert e.set_tuning(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=2).targets_per_thread == 2
+        for scale, tpt in ((1.0, 2), (0.7, 1), (1.0, 2)):
+            xl = [t * scale for t in L]
+            e.set_box(xl)
+            x = w.x * scale
+            e.set_state(x=x)
+            s = e.accel(True)
+            assert e.tuning().targets_per_thread == tpt, scale
+            p2 = w.yk_params(precision=prec)
+            for k in range(3):
+                p2.xl[k] = xl[k]
+            a_ref, s_ref = orc.accel(p2, x, w.zii, w.aii, True)
+            tol = FP64_TOL if prec == abi.YK_PREC_FP64 else MIX_F_TOL
+            assert rel_norm(e.a[:3 * w.n], a_ref[:3 * w.n]) <= tol
+            assert rel(s.ev, s_ref.ev) <= (FP64_TOL if prec == abi.YK_PREC_FP64 else MIX_S_TOL)
+    wn = configs.nucleon_matter(82, 2000)
+    with Engine(wn.yk_params(precision=prec), wn.x, wn.v, wn.zii, wn.aii) as e:
+        assert e.set_tuning(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=2).targets_per_thread == 1
+
+
 def test_kernels_actually_launch(gpu):
     w = configs.pure_ion_ocp(71, 300)
     before = kernel_launch_count()
@@ -274,7 +354,7 @@ def _reshaped(w, stretch, rccut=None):
     return w2
 
 
-@pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
+@pytest.mark.parametrize("kern", ["rows", "pairs", "near", "pairs-tpt2"])
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
 @pytest.mark.parametrize("case", ["rectangular", "cutoff-at-half-box", "no-cutoff"])
 def test_box_shapes_and_cutoffs(gpu, orc, case, prec, kern):

@@ -4,7 +4,9 @@ no GPU).  Every unit (R, C), C >= R, of the half-pair sum must be in exactly
 one job, or a pair is lost or counted twice; jobs must respect the cap and
 the guided sizes d <= max(1, W / 2P), W the work not yet handed out; and the
 Si slots of a row must be 0 .. row_slots[R] - 1, each written once, because
-k_combine sums exactly those."""
+k_combine sums exactly those.  The two-target table (build_pair_jobs2, read
+through yk_pair_jobs2) must cover every unit of both rows of each block
+pair exactly once and give both rows the same slots."""
 import numpy as np
 import pytest
 
@@ -49,3 +51,23 @@ def test_small_box_is_one_job():
 def test_bad_arguments(m, cap, ctas):
     with pytest.raises(ValueError):
         pair_jobs(m, cap, ctas)
+
+
+@pytest.mark.parametrize("m,cap,ctas", [(1, 8, 592), (2, 8, 592), (3, 4, 592), (5, 1, 592), (33, 8, 592),
+                                        (432, 8, 592), (432, 4, 592), (701, 16, 296)])
+def test_two_target_jobs_cover_every_unit_once(m, cap, ctas):
+    jobs, slots = pair_jobs(m, cap, ctas, targets_per_thread=2)
+    R, C0, C1, s = jobs.T.astype(np.int64)
+    assert np.all(R % 2 == 0) and np.all(C0 >= R) and np.all(C1 > C0) and np.all(C1 <= m)
+    assert np.all(C1 - C0 <= cap)
+    cover = np.zeros((m, m), dtype=np.int64)
+    for r, a, b in zip(R, C0, C1):
+        cover[r, a:b] += 1                      # block R: tiles C >= R
+        if r + 1 < m:
+            cover[r + 1, max(a, r + 1):b] += 1  # block R + 1: tiles C >= R + 1
+    assert np.array_equal(cover, np.triu(np.ones((m, m), dtype=np.int64)))
+    for r in range(0, m, 2):
+        mine = np.sort(s[R == r])
+        assert np.array_equal(mine, np.arange(slots[r]))
+        if r + 1 < m:
+            assert slots[r + 1] == slots[r]

@@ -60,6 +60,8 @@ SIGNATURES = {
     "yk_peak_probe": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "yk_pair_jobs": (C.c_longlong, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_longlong,
                                     C.POINTER(C.c_int)]),
+    "yk_pair_jobs2": (C.c_longlong, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_longlong,
+                                     C.POINTER(C.c_int)]),
     "yk_accel_noalloc": (C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p, _S, C.c_void_p]),
     "yk_wait_selftest": (C.c_int, [_ctx, C.c_longlong, C.POINTER(C.c_int)]),

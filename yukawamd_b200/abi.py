@@ -113,6 +113,7 @@ class YkTuning(C.Structure):
         ("sort_every", C.c_int),
         ("graph_steps", C.c_int),
         ("source_split", C.c_int),
+        ("targets_per_thread", C.c_int),
     ]
 
 

@@ -942,6 +942,7 @@ int yk_batch_get_tuning(yk_batch* b, yk_tuning* out)
     out->sort_every = b->graph_steps;       // the batch re-sorts at the start of every graph
     out->graph_steps = b->graph_steps;
     out->source_split = 1;
+    out->targets_per_thread = 1;
     return YK_OK;
 }
 
@@ -952,6 +953,8 @@ int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t)
         return bfail(b, YK_ERR_UNSUPPORTED, "a batch runs the half-pair kernel (force_kernel 0 or 2)");
     if (t->pair_seg < 0 || t->graph_steps < 0) return bfail(b, YK_ERR_ARG, "bad tuning values");
     if (t->source_split > 1) return bfail(b, YK_ERR_UNSUPPORTED, "a batch runs whole source tiles (source_split 0 or 1)");
+    if (t->targets_per_thread > 1)
+        return bfail(b, YK_ERR_UNSUPPORTED, "a batch runs one target per thread (targets_per_thread 0 or 1)");
     BCK(b, cudaSetDevice(b->dev));
     BCK(b, cudaStreamSynchronize(b->stream));
     drop_graphs_b(b);

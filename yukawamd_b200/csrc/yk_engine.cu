@@ -25,6 +25,7 @@
 #include "yk_force.cuh"
 #include "yk_internal.h"
 #include "yk_pairs.cuh"
+#include "yk_pairs2.cuh"
 #include "yk_gofr.cuh"
 #include "yk_near.cuh"
 #include "yk_sort.cuh"
@@ -169,6 +170,8 @@ struct yk_ctx {
     int kernel_req = 0;             // as requested (0 = auto)
     int seg = DEFAULT_SEG;
     int split = 1;                  // CTAs per unit of the half-pair kernel (yk_tuning.source_split)
+    int tpt_req = 0;                // targets per thread as requested (yk_tuning.targets_per_thread; 0 auto)
+    int pj_tt = 1;                  // targets per thread the job table was built for (pair_tt)
     bool seg_auto = true;           // pair_seg not set by the caller: the precision's default
     int sort_every = DEFAULT_SORT_EVERY;
     int graph_steps = DEFAULT_GRAPH_STEPS;
@@ -413,9 +416,66 @@ static void build_split_jobs(int M, int split, std::vector<int4>& jobs, std::vec
                 jobs.push_back(make_int4(R, C, C + 1, row_slots[R]++ | (part << 20) | (lg << 24)));
 }
 
+// Jobs of k_force_pairs2 (two targets per thread) for M tiles: a job
+// (R, C0, C1, s), R even, takes source tiles C0 <= C < C1 (C >= R) against
+// blocks R and R + 1 and writes Si slot s of both rows.  The same guided
+// self-scheduling as build_pair_jobs over the block pairs, a tile of a pair
+// counting one CTA tile step; row_slots of both rows count the pair's jobs.
+static void build_pair_jobs2(int M, int smax, int P, std::vector<int4>& jobs, std::vector<int>& row_slots)
+{
+    jobs.clear();
+    row_slots.assign(M, 0);
+    const int np = (M + 1) / 2;
+    std::vector<int> done(np, 0), cnt(np, 0);
+    long long W = 0;
+    std::priority_queue<std::pair<int, int>> rows;          // (tiles left, -pair)
+    for (int p = 0; p < np; ++p) {
+        W += M - 2 * p;
+        rows.push(std::make_pair(M - 2 * p, -p));
+    }
+    while (!rows.empty()) {
+        const int left = rows.top().first, p = -rows.top().second;
+        rows.pop();
+        const long long want = W / (2LL * std::max(P, 1));
+        const int d = (int)std::min<long long>(left, std::min<long long>(smax, std::max<long long>(1, want)));
+        const int R = 2 * p, C0 = R + done[p];
+        jobs.push_back(make_int4(R, C0, C0 + d, cnt[p]++));
+        done[p] += d;
+        W -= d;
+        if (left > d) rows.push(std::make_pair(left - d, -p));
+    }
+    for (int p = 0; p < np; ++p) {
+        row_slots[2 * p] = cnt[p];
+        if (2 * p + 1 < M) row_slots[2 * p + 1] = cnt[p];
+    }
+}
+
+// Targets per thread of the half-pair kernel for the context as it stands:
+// 2 (k_force_pairs2) for ion boxes on the paths that kernel has (FP64 with
+// exact screen images, mixed with the hi/lo displacement) when requested,
+// else 1.  Automatic (0): 2 for mixed-form ion boxes of TPT2_AUTO_MIN_N
+// particles or more.  Measured on a B200 (force call, CUDA events): the
+// 55,296-ion mixture mixed 1.050 -> 1.004 ms with two targets (jobs of up
+// to 8 tiles), FP64 2.21 -> 2.46 ms (four CTAs per SM instead of five, and
+// the larger warp boxes evaluate more masked pairs); the 4,096-ion OCP mixed
+// 0.046 -> 0.048 ms (too few jobs).
+constexpr int TPT2_AUTO_MIN_N = 16384;
+constexpr int DEFAULT_SEG_MIXED_TT2 = 8;
+
+static int pair_tt(const yk_ctx* c)
+{
+    if (c->split > 1 || c->kernel_req == 3) return 1;
+    if (c->p.sim_type != YK_SIM_PURE_ION && c->p.sim_type != YK_SIM_ION_MIXTURE) return 1;
+    const bool mixed = c->p.precision == YK_PREC_MIXED;
+    const int want = c->tpt_req != 0 ? c->tpt_req : ((mixed && c->n >= TPT2_AUTO_MIN_N) ? 2 : 1);
+    if (want != 2) return 1;
+    return (mixed ? c->fa.lo : c->fa.img_k) ? 2 : 1;
+}
+
 static int auto_pair_seg(const yk_ctx* c)
 {
-    return c->p.precision == YK_PREC_MIXED ? DEFAULT_SEG_MIXED : DEFAULT_SEG_FP64;
+    if (c->p.precision == YK_PREC_MIXED) return pair_tt(c) == 2 ? DEFAULT_SEG_MIXED_TT2 : DEFAULT_SEG_MIXED;
+    return DEFAULT_SEG_FP64;
 }
 
 // Resident CTAs of the half-pair kernels on a device (6 per SM), for the job
@@ -475,7 +535,9 @@ static int setup_pairs(yk_ctx* c)
     std::vector<int4> jobs;
     std::vector<int> slots;
     // the near-list kernel reads whole tiles: no split for it
+    c->pj_tt = pair_tt(c);
     if (c->split > 1 && c->kernel_req != 3) build_split_jobs(M, c->split, jobs, slots);
+    else if (c->pj_tt == 2) build_pair_jobs2(M, c->seg, pair_ctas(c->dev) * 4 / 6, jobs, slots);
     else build_pair_jobs(M, c->seg, pair_ctas(c->dev), jobs, slots);
     const int nseg = M > 0 ? *std::max_element(slots.begin(), slots.end()) : 0;
     const size_t units = (size_t)M * (M + 1) / 2;
@@ -495,6 +557,18 @@ static int setup_pairs(yk_ctx* c)
     c->pj.nseg_max = nseg;
     c->pj.tbox = c->tbox;
     c->pj.Sjf = c->Sjf;
+    return YK_OK;
+}
+
+// A new box can change whether k_force_pairs2 applies (fa.img_k, fa.lo):
+// rebuild the job table when it does.
+static int refresh_pair_tt(yk_ctx* c)
+{
+    if (c->kernel == 2 && pair_tt(c) != c->pj_tt) {
+        CK(c, cudaSetDevice(c->dev));
+        CK(c, cudaStreamSynchronize(c->stream));
+        return setup_pairs(c);
+    }
     return YK_OK;
 }
 
@@ -607,6 +681,19 @@ static int launch_force_t(yk_ctx* c)
         const int grid = persistent_grid<k_force_near<SIM, PREC, MEAS>>(c->dev);
         k_force_near<SIM, PREC, MEAS><<<std::min(grid, njobs), PB, 0, c->stream>>>(
             c->pos, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
+    } else if (c->pj_tt == 2) {
+        // two targets per thread: ion boxes with fa.lo (mixed) or fa.img_k (FP64) only (pair_tt)
+        if constexpr (SIM != SIM_NUCLEON) {
+            if (pairs_tile_boxes<SIM, PREC, PREC == PREC_MIXED>()) {
+                k_tile_boxes<<<c->pj.M, PB, 0, c->stream>>>(c->posf, c->n, c->fa, c->tbox);
+                ++k;
+            } else {
+                pj.tbox = nullptr;
+            }
+            const int grid = persistent_grid<k_force_pairs2<SIM, PREC, MEAS>>(c->dev);
+            k_force_pairs2<SIM, PREC, MEAS><<<std::min(grid, njobs), PB, 0, c->stream>>>(
+                c->pos, c->posf, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
+        }
     } else {
         if (lo_path<SIM, PREC>(c->fa) && pairs_tile_boxes<SIM, PREC, true>()) {
             k_tile_boxes<<<c->pj.M, PB, 0, c->stream>>>(c->posf, c->n, c->fa, c->tbox);
@@ -883,6 +970,9 @@ extern "C" {
 
 const char* yk_version(void) { return YK_VERSION_STR; }
 
+static long long copy_jobs(const std::vector<int4>& list, const std::vector<int>& slots, int* jobs,
+                           long long max_jobs, int* row_slots);
+
 long long yk_pair_jobs(int m, int cap, int ctas, int* jobs, long long max_jobs, int* row_slots)
 {
     if (m < 1 || cap < 1 || ctas < 1 || max_jobs < 0 || (jobs == nullptr && max_jobs > 0))
@@ -890,6 +980,22 @@ long long yk_pair_jobs(int m, int cap, int ctas, int* jobs, long long max_jobs, 
     std::vector<int4> list;
     std::vector<int> slots;
     build_pair_jobs(m, cap, ctas, list, slots);
+    return copy_jobs(list, slots, jobs, max_jobs, row_slots);
+}
+
+long long yk_pair_jobs2(int m, int cap, int ctas, int* jobs, long long max_jobs, int* row_slots)
+{
+    if (m < 1 || cap < 1 || ctas < 1 || max_jobs < 0 || (jobs == nullptr && max_jobs > 0))
+        return -(long long)YK_ERR_ARG;
+    std::vector<int4> list;
+    std::vector<int> slots;
+    build_pair_jobs2(m, cap, ctas, list, slots);
+    return copy_jobs(list, slots, jobs, max_jobs, row_slots);
+}
+
+static long long copy_jobs(const std::vector<int4>& list, const std::vector<int>& slots, int* jobs,
+                           long long max_jobs, int* row_slots)
+{
     const long long k = std::min<long long>(max_jobs, (long long)list.size());
     for (long long j = 0; j < k; ++j) {
         jobs[4 * j] = list[j].x;
@@ -1103,6 +1209,7 @@ int yk_get_tuning(yk_ctx* c, yk_tuning* out)
     out->sort_every = c->sort_every;
     out->graph_steps = c->graph_steps;
     out->source_split = c->kernel == 2 ? c->split : 1;
+    out->targets_per_thread = c->kernel == 2 ? c->pj_tt : 1;
     return YK_OK;
 }
 
@@ -1114,7 +1221,10 @@ int yk_set_tuning(yk_ctx* c, const yk_tuning* t)
         return fail(c, YK_ERR_ARG, "bad tuning values");
     if (t->source_split != 0 && t->source_split != 1 && t->source_split != 2 && t->source_split != 4)
         return fail(c, YK_ERR_ARG, "source_split must be 0, 1, 2 or 4");
+    if (t->targets_per_thread < 0 || t->targets_per_thread > 2)
+        return fail(c, YK_ERR_ARG, "targets_per_thread must be 0, 1 or 2");
     c->split = t->source_split > 1 ? t->source_split : 1;
+    c->tpt_req = t->targets_per_thread;
     CK(c, cudaSetDevice(c->dev));
     CK(c, cudaStreamSynchronize(c->stream));
     drop_graphs(c);
@@ -1411,7 +1521,7 @@ int yk_set_box(yk_ctx* c, const double xl[3])
     for (int k = 0; k < 3; ++k) c->p.xl[k] = xl[k];
     setup_args(c);
     drop_graphs(c);
-    return YK_OK;
+    return refresh_pair_tt(c);
 }
 
 // ---- gen_utils.f / strain.f on the device ---------------------------------
@@ -1522,6 +1632,8 @@ int yk_strain(yk_ctx* c, const double deps[3], const double xl0[3], double xl_ou
         for (int k = 0; k < 3; ++k) c->p.xl[k] = xl[k];
         setup_args(c);
         drop_graphs(c);
+        const int rc = refresh_pair_tt(c);
+        if (rc) return rc;
     }
     c->pos_dirty = true;
     if (xl_out)

@@ -534,16 +534,16 @@ __device__ __forceinline__ float warp_maxf(float v)
     return v;
 }
 
-__device__ __forceinline__ WarpBox warp_box(const ForceArgs& fa, const double4& pi, bool active)
+// The warp's box from each lane's lower and upper corner (+inf / -inf for a
+// lane without active targets).
+__device__ __forceinline__ WarpBox warp_box_of(const ForceArgs& fa, const float (&lo)[3], const float (&hi)[3],
+                                               bool active, bool proton)
 {
     WarpBox b;
-    const float inf = __int_as_float(0x7f800000);
-    const double c[3] = {pi.x, pi.y, pi.z};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float v = __double2float_rn(c[k]);
-        b.lo[k] = warp_minf(active ? v : inf);
-        b.hi[k] = warp_maxf(active ? v : -inf);
+        b.lo[k] = warp_minf(lo[k]);
+        b.hi[k] = warp_maxf(hi[k]);
         // margin: 2^-18 L for the FP32 arithmetic (the box, its centre and
         // the source's minimum image are each a few roundings of values below
         // L) plus 2 SHADOW_Q for the grid rounding of the shadow coordinate
@@ -552,7 +552,7 @@ __device__ __forceinline__ WarpBox warp_box(const ForceArgs& fa, const double4& 
         b.h[k] = fmaf(0.5f, b.hi[k] - b.lo[k], mu);
     }
     b.any = __any_sync(0xffffffffu, active);
-    b.has_p = __any_sync(0xffffffffu, active && pi.w == 1.0);
+    b.has_p = __any_sync(0xffffffffu, proton);
     // A pair inside r_c has |d| <= r_c < L/2 per axis in its minimum image.
     // Seen from the centre, a reachable source lies within r_c + h per axis
     // of the image k that the centre gives it, and a target within h, so the
@@ -568,6 +568,21 @@ __device__ __forceinline__ WarpBox warp_box(const ForceArgs& fa, const double4& 
     }
     b.tile_img = ok;
     return b;
+}
+
+// The box of a warp with one target per lane.
+__device__ __forceinline__ WarpBox warp_box(const ForceArgs& fa, const double4& pi, bool active)
+{
+    const float inf = __int_as_float(0x7f800000);
+    const double c[3] = {pi.x, pi.y, pi.z};
+    float lo[3], hi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float v = __double2float_rn(c[k]);
+        lo[k] = active ? v : inf;
+        hi[k] = active ? v : -inf;
+    }
+    return warp_box_of(fa, lo, hi, active, active && pi.w == 1.0);
 }
 
 // Lower bound of the minimum-image distance^2 from source (x, w) to the box:

@@ -172,11 +172,11 @@ class Engine:
         return t
 
     def set_tuning(self, force_kernel=None, pair_seg=None, sort_every=None, graph_steps=None,
-                   source_split=None):
+                   source_split=None, targets_per_thread=None):
         t = self.tuning()
         for name, val in (("force_kernel", force_kernel), ("pair_seg", pair_seg),
                           ("sort_every", sort_every), ("graph_steps", graph_steps),
-                          ("source_split", source_split)):
+                          ("source_split", source_split), ("targets_per_thread", targets_per_thread)):
             if val is not None:
                 setattr(t, name, int(val))
         check(self._lib.yk_set_tuning(self._ctx, C.byref(t)), self._ctx)
@@ -367,17 +367,19 @@ def peak_probe(device=0, kind=0):
     return out.value
 
 
-def pair_jobs(m, cap, ctas):
-    """The half-pair kernel's job table for m tiles (yk_pair_jobs): an int
-    array of shape (jobs, 4) with rows (R, C0, C1, slot) in dispatch order,
-    and the Si slot count of every row.  Host arithmetic only."""
-    k = lib().yk_pair_jobs(int(m), int(cap), int(ctas), None, 0, None)
+def pair_jobs(m, cap, ctas, targets_per_thread=1):
+    """The half-pair kernel's job table for m tiles (yk_pair_jobs, or
+    yk_pair_jobs2 for two targets per thread): an int array of shape (jobs, 4)
+    with rows (R, C0, C1, slot) in dispatch order, and the Si slot count of
+    every row.  Host arithmetic only."""
+    fn = lib().yk_pair_jobs2 if targets_per_thread == 2 else lib().yk_pair_jobs
+    k = fn(int(m), int(cap), int(ctas), None, 0, None)
     if k < 0:
         raise ValueError("yk_pair_jobs: bad arguments (m=%r, cap=%r, ctas=%r)" % (m, cap, ctas))
     jobs = np.zeros((k, 4), dtype=np.int32)
     slots = np.zeros(int(m), dtype=np.int32)
-    got = lib().yk_pair_jobs(int(m), int(cap), int(ctas), jobs.ctypes.data_as(C.POINTER(C.c_int)), k,
-                             slots.ctypes.data_as(C.POINTER(C.c_int)))
+    got = fn(int(m), int(cap), int(ctas), jobs.ctypes.data_as(C.POINTER(C.c_int)), k,
+             slots.ctypes.data_as(C.POINTER(C.c_int)))
     assert got == k
     return jobs, slots
 

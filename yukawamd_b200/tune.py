@@ -5,7 +5,9 @@ kernel with scratch, the same over per-warp near-source lists, or the row
 kernel that evaluates each pair from both sides), cap the half-pair jobs at
 `pair_seg` source tiles (the job list shrinks them towards its end), let
 1, 2 or 4 CTAs share each 128-target block (`source_split`: the threads per
-target, for small boxes); it refreshes
+target, for small boxes), give each thread one or two targets
+(`targets_per_thread`: target blocks of 128 or 256 slots, the tile shape of
+the ion kernels); it refreshes
 the Morton order every `sort_every` steps.  Which choice is fastest depends on
 N, the cutoff radius relative to the box, the interaction and the precision,
 so the tuner measures candidates on the caller's own workload (CUDA-event
@@ -37,6 +39,11 @@ CANDIDATES = [
     # threads per target: 2 or 4 CTAs share each 128-target block (small boxes)
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=50, source_split=2),
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=50, source_split=4),
+    # tile shape: two targets per thread (256-target blocks; ion boxes on the
+    # FP64 exact-image or mixed hi/lo path, others fall back to one)
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=50, targets_per_thread=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=4, sort_every=50, targets_per_thread=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=16, sort_every=50, targets_per_thread=2),
 ]
 # source_split > 1 makes one job per unit and part: only worth trying while the
 # box has few tiles (it is there to fill the GPU with a small box)
@@ -108,6 +115,7 @@ def tune(engine, candidates=None, steps=6, warmup=2, device=0, save=True):
     for cand in candidates:
         cand = dict(cand)
         cand.setdefault("source_split", 1)
+        cand.setdefault("targets_per_thread", 1)
         try:
             ms = measure(engine, cand, steps, warmup)
         except Exception as exc:          # e.g. scratch too large for this N
@@ -173,6 +181,6 @@ def apply(engine, device=0):
     ent = _load().get(key_for(engine, device))
     if not ent:
         return False
-    engine.set_tuning(**{k: ent[k] for k in ("force_kernel", "pair_seg", "sort_every", "source_split")
-                         if k in ent})
+    engine.set_tuning(**{k: ent[k] for k in ("force_kernel", "pair_seg", "sort_every", "source_split",
+                                             "targets_per_thread") if k in ent})
     return True
