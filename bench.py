@@ -438,8 +438,8 @@ def run_ours(args, dist):
            "config": {"workload": workload_desc(w, kind), "n": w.n,
                       "pairs_per_step": pairs_step, "precision": args.precision,
                       "integrator": "vel_verlet_2", "meas_every": me,
-                      "l2": "flushed: 256 MiB device memset before every timed step "
-                            "(inside the timed region)",
+                      "l2": "flushed: 256 MiB device memset between timed steps (each step "
+                            "timed by its own CUDA-event pair after the flush)",
                       "parallelism": "replicas x%d (one box per GPU, no collective)" % dist.world},
            "roofline": roofline, "gpu_launches": launches, "clocks": clk}
     e.close()

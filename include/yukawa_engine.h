@@ -344,7 +344,8 @@ YK_API int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t);
  * since the last enable.
  */
 typedef struct yk_perf {
-    double run_ms;            /* event time of the yk_run calls           */
+    double run_ms;            /* event time of the timed steps, each from
+                                 the end of its L2 flush to its end       */
     double force_ms;          /* event time of the force kernels          */
     long long steps;          /* integrator steps timed                   */
     long long force_calls;    /* force kernels timed                      */

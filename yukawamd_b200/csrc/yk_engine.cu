@@ -1357,27 +1357,36 @@ int yk_run(yk_ctx* c, int nsteps, int meas_every, yk_scalars* series)
     auto meas_at = [&](int s) { return me > 0 && s % me == 0; };
     int k = 0;
     if (c->perf_on) {
-        // Timed path: step by step, event pairs around every force call.
+        // Timed path: step by step, an event pair around every step (after
+        // its L2 flush, so the flush lies between timed steps) and one
+        // around every force call inside it.
         c->ev_used = 0;
-        cudaEvent_t e0 = next_event(c), e1 = next_event(c);
-        CK(c, cudaEventRecord(e0, c->stream));
+        std::vector<int> step_ev;
+        step_ev.reserve(2 * (size_t)nsteps);
         for (int s = 1; s <= nsteps; ++s) {
             if (c->flush_bytes)
                 CK(c, cudaMemsetAsync(c->flush_buf, s & 0xff, c->flush_bytes, c->stream));
+            step_ev.push_back(c->ev_used);
+            CK(c, cudaEventRecord(next_event(c), c->stream));
             k += enqueue_newton(c, meas_at(s), want_series, sort_due(c, c->step_count), true);
             c->step_count += 1;
+            step_ev.push_back(c->ev_used);
+            CK(c, cudaEventRecord(next_event(c), c->stream));
         }
-        CK(c, cudaEventRecord(e1, c->stream));
         g_launches += k;
         int rc = sync_and_check(c);
         if (rc) return rc;
         float ms = 0.f;
-        CK(c, cudaEventElapsedTime(&ms, e0, e1));
-        c->perf.run_ms += ms;
-        for (int q = 2; q + 1 < c->ev_used; q += 2) {
-            CK(c, cudaEventElapsedTime(&ms, c->ev_pool[q], c->ev_pool[q + 1]));
-            c->perf.force_ms += ms;
-            c->perf.force_calls += 1;
+        for (int s = 0; s < nsteps; ++s) {
+            const int a = step_ev[2 * s], b = step_ev[2 * s + 1];
+            CK(c, cudaEventElapsedTime(&ms, c->ev_pool[a], c->ev_pool[b]));
+            c->perf.run_ms += ms;
+            // the force calls' event pairs lie between the step's own two
+            for (int q = a + 1; q + 1 < b; q += 2) {
+                CK(c, cudaEventElapsedTime(&ms, c->ev_pool[q], c->ev_pool[q + 1]));
+                c->perf.force_ms += ms;
+                c->perf.force_calls += 1;
+            }
         }
         c->perf.steps += nsteps;
         return finish_run(c, nsteps, want_series, series);
