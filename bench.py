@@ -589,6 +589,8 @@ def nucleon_pair(K, W, me, dist):
         res["force_rms_rel_err_vs_fp64"] = float(np.linalg.norm(a32.a[:3 * n] - a64.a[:3 * n]) /
                                                  np.linalg.norm(a64.a[:3 * n]))
         res["ev_rel_err"] = abs(s32.ev - s64.ev) / abs(s64.ev)
+    if dist.rank == 0 and dist.world == 1:
+        res["mixed_vs_oracle"] = mixed_vs_oracle(w)
     return res
 
 
