@@ -266,7 +266,10 @@ def time_engine(w, precision, steps, warmup, meas_every, dist, flush=True):
     e = Engine(w, precision=prec, device=dist.local)
     if KERNEL_CHOICE[0]:
         e.set_tuning(force_kernel=KERNEL_CHOICE[0])
-    e.kernel_name = {1: "k_force_rows", 2: "k_force_pairs", 3: "k_force_near"}.get(e.tuning().force_kernel, "?")
+    t = e.tuning()
+    e.kernel_name = {1: "k_force_rows", 2: "k_force_pairs", 3: "k_force_near"}.get(t.force_kernel, "?")
+    if t.force_kernel == 2 and t.targets_per_thread == 2:
+        e.kernel_name = "k_force_pairs2"
     e.accel(True)                                  # md.F:69, initial forces
     if warmup:
         e.run(warmup, meas_every, series=False)
@@ -465,6 +468,19 @@ def run_ours(args, dist):
                       "ratio_mixed_over_fp64": (v2 / value) if other == "mixed" else (value / v2),
                       "force_rms_rel_err_vs_fp64": ferr, "ev_rel_err": ev_err,
                       "px_rel_err": px_err}
+        # the companion's force kernel against its own pipe's measured peak
+        kind2 = 1 if other == "mixed" else 0
+        fms2 = perf2.force_ms / max(perf2.force_calls, 1)
+        ach2 = fpp * pairs_step / (fms2 * 1e-3) / 1e12
+        peak2 = peak_probe(dist.local, kind2)
+        out[other]["roofline"] = {"bound": "fp32" if kind2 else "fp64", "achieved": ach2, "peak": peak2,
+                                  "unit": "TFLOP/s", "frac": ach2 / peak2,
+                                  "traffic": read_traffic(kind, other),
+                                  "kernel": "%s + k_combine (force call), avg %.3f ms/launch over %d launches"
+                                            % (e2.kernel_name, fms2, perf2.force_calls),
+                                  "peak_source": "measured live by yk_peak_probe (%s FMA chain, all SMs)"
+                                                 % ("FP32" if kind2 else "FP64"),
+                                  "flops_per_pair": fpp}
         e2.close()
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
             out["mixed"]["vs_oracle"] = mixed_vs_oracle(w)

@@ -321,6 +321,35 @@ def test_two_targets_per_thread_follows_the_box(gpu, orc, prec):
         assert e.set_tuning(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=2).targets_per_thread == 1
 
 
+@pytest.mark.parametrize("tpt", [1, 2], ids=["tpt1", "tpt2"])
+@pytest.mark.parametrize("kind", ["pure", "mix"])
+def test_mixed_displacement_large_box(gpu, orc, kind, tpt):
+    """The mixed form's FP32 ion displacement (hi parts on the 2^-9 fm grid,
+    exact differences, a lo correction) in a box of L = 16,000 fm, just inside
+    the limit for it (every coordinate below 16,384 fm), with particles
+    crowded against both faces so that the hi parts are as large as they get
+    and many pairs cross the periodic boundary: forces within 1e-6 RMS and
+    ev, px within 1e-6 of the FP64 oracle; the FP64 form within 1e-12."""
+    import copy
+    w = copy.deepcopy(workload(kind, 3000, 900 + tpt))
+    L = 16000.0
+    rng = np.random.default_rng(77)
+    X = rng.random((w.n, 3))
+    # half the particles within 500 fm of a face (either side)
+    edge = rng.random(w.n) < 0.5
+    X[edge] = np.where(rng.random((edge.sum(), 3)) < 0.5, X[edge] * (500.0 / L), 1.0 - X[edge] * (500.0 / L))
+    w.x = np.ascontiguousarray((X * L).reshape(-1))
+    w.params["xl"] = [L, L, L]
+    w.params["rccut"] = 0.35 * L
+    w.params["xmuc"] = 1.0 / 1500.0
+    for prec in (abi.YK_PREC_FP64, abi.YK_PREC_MIXED):
+        p = w.yk_params(precision=prec)
+        with Engine(p, w.x, w.v, w.zii, w.aii) as e:
+            t = e.set_tuning(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=tpt)
+            assert t.targets_per_thread == tpt
+        check_accel(orc, w, prec, True, tuning=dict(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=tpt))
+
+
 def test_kernels_actually_launch(gpu):
     w = configs.pure_ion_ocp(71, 300)
     before = kernel_launch_count()
