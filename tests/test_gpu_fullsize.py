@@ -101,9 +101,18 @@ def _rows_nearest_half_box(w, count):
 
 @pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
 def test_nucleons_51200_every_particle(gpu, nuc_ref, prec):
+    _check_nucleons(nuc_ref, prec, 1)
+
+
+def test_nucleons_51200_two_targets_per_thread(gpu, nuc_ref):
+    _check_nucleons(nuc_ref, abi.YK_PREC_MIXED, 2)
+
+
+def _check_nucleons(nuc_ref, prec, tpt):
     w, a_ref, s_ref = nuc_ref
     n = w.n
     with Engine(w.yk_params(precision=prec), w.x, w.v, w.zii, w.aii) as e:
+        assert e.set_tuning(targets_per_thread=tpt).targets_per_thread == tpt
         s = e.accel(True)
         a = e.a.copy()
     _check(a, s, a_ref, s_ref, n, prec)
@@ -128,8 +137,9 @@ def _half_box_pairs(seed, n, L, deltas):
     return np.ascontiguousarray(np.mod(X, L).reshape(-1))
 
 
-@pytest.mark.parametrize("prec", [abi.YK_PREC_FP64, abi.YK_PREC_MIXED], ids=["fp64", "mixed"])
-def test_image_decisions_at_half_box(gpu, orc, prec):
+@pytest.mark.parametrize("prec,tpt", [(abi.YK_PREC_FP64, 1), (abi.YK_PREC_MIXED, 1), (abi.YK_PREC_MIXED, 2)],
+                         ids=["fp64", "mixed", "mixed-tpt2"])
+def test_image_decisions_at_half_box(gpu, orc, prec, tpt):
     L, n = 30.0, 400
     base = [0.0, 1e-13, -1e-13, 1e-9, -1e-9, 1e-7, -1e-7, 1e-6, -1e-6, 1e-5, -1e-5, 1e-4, -1e-4,
             1e-3, -1e-3, 3e-3, -3e-3]
@@ -142,6 +152,7 @@ def test_image_decisions_at_half_box(gpu, orc, prec):
     zii = np.ones(n)
     aii = np.ones(n)
     with Engine(p, x, np.zeros(3 * n), zii, aii) as e:
+        assert e.set_tuning(targets_per_thread=tpt).targets_per_thread == tpt
         e.accel(True)
         a = e.a[:3 * n].copy()
     a_ref, _ = orc.accel(p, x, zii, aii, True)

@@ -285,6 +285,22 @@ def test_two_targets_per_thread_ragged(gpu, orc, kind, n):
         check_tpt2(orc, w, prec, False, "tpt2-seg1")
 
 
+@pytest.mark.parametrize("kern", list(TPT2))
+@pytest.mark.parametrize("meas", [True, False], ids=["meas", "force"])
+@pytest.mark.parametrize("n", [3000, 6001])
+def test_two_targets_per_thread_nucleons(gpu, orc, n, meas, kern):
+    """Nucleons, mixed form (the hi/lo displacement with the flagged exact
+    image near L/2): the two-target kernel against the oracle."""
+    check_tpt2(orc, workload("nn", n, 500 + n), abi.YK_PREC_MIXED, meas, kern)
+
+
+@pytest.mark.parametrize("n", [1, 2, 17, 128, 129, 255, 257, 383, 385])
+def test_two_targets_per_thread_nucleons_ragged(gpu, orc, n):
+    w = workload("nn", n, 31 + n)
+    check_tpt2(orc, w, abi.YK_PREC_MIXED, True, "tpt2")
+    check_tpt2(orc, w, abi.YK_PREC_MIXED, False, "tpt2-seg1")
+
+
 @pytest.mark.parametrize("mode", [abi.YK_MIX_COMPAT, abi.YK_MIX_FIXED], ids=["compat", "fixed"])
 def test_two_targets_per_thread_mix_modes(gpu, orc, mode):
     w = _short_cutoff(workload("mix", 513, 5), 0.4)
@@ -296,7 +312,7 @@ def test_two_targets_per_thread_follows_the_box(gpu, orc, prec):
     """targets_per_thread = 2 runs on ion boxes whose screen images are exact;
     a box change that breaks that condition (the cutoff beyond L/2) takes the
     one-target kernel, and a change back returns to two; the forces match the
-    oracle throughout.  Nucleon boxes always report 1."""
+    oracle throughout.  Nucleon boxes report 2 in the mixed form only."""
     w = _short_cutoff(configs.ion_mixture_cfg(81, 3000), 0.4)
     p = w.yk_params(precision=prec)
     L = list(p.xl)
@@ -318,7 +334,9 @@ def test_two_targets_per_thread_follows_the_box(gpu, orc, prec):
             assert rel(s.ev, s_ref.ev) <= (FP64_TOL if prec == abi.YK_PREC_FP64 else MIX_S_TOL)
     wn = configs.nucleon_matter(82, 2000)
     with Engine(wn.yk_params(precision=prec), wn.x, wn.v, wn.zii, wn.aii) as e:
-        assert e.set_tuning(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=2).targets_per_thread == 1
+        # nucleons: two targets in the mixed form only
+        want = 2 if prec == abi.YK_PREC_MIXED else 1
+        assert e.set_tuning(force_kernel=abi.KERNEL_PAIRS, targets_per_thread=2).targets_per_thread == want
 
 
 @pytest.mark.parametrize("tpt", [1, 2], ids=["tpt1", "tpt2"])

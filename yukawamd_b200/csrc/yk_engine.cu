@@ -458,15 +458,22 @@ static void build_pair_jobs2(int M, int smax, int P, std::vector<int4>& jobs, st
 // 55,296-ion mixture mixed 1.050 -> 1.004 ms with two targets (jobs of up
 // to 8 tiles), FP64 2.21 -> 2.46 ms (four CTAs per SM instead of five, and
 // the larger warp boxes evaluate more masked pairs); the 4,096-ion OCP mixed
-// 0.046 -> 0.048 ms (too few jobs).
+// 0.046 -> 0.048 ms (too few jobs); the 51,200-nucleon box mixed 1.15 ->
+// 1.40 ms (its one-target kernel runs 7 CTAs per SM, and 64-nucleon warp
+// boxes are large against the 11.5 fm nuclear cutoff), so nucleons take two
+// targets only when asked (the tuner tries it).
 constexpr int TPT2_AUTO_MIN_N = 16384;
 constexpr int DEFAULT_SEG_MIXED_TT2 = 8;
 
 static int pair_tt(const yk_ctx* c)
 {
     if (c->split > 1 || c->kernel_req == 3) return 1;
-    if (c->p.sim_type != YK_SIM_PURE_ION && c->p.sim_type != YK_SIM_ION_MIXTURE) return 1;
     const bool mixed = c->p.precision == YK_PREC_MIXED;
+    if (c->p.sim_type == YK_SIM_NUCLEON) {
+        // nucleons: the mixed form on the hi/lo displacement only
+        return (c->tpt_req == 2 && mixed && c->fa.hilo) ? 2 : 1;
+    }
+    if (c->p.sim_type != YK_SIM_PURE_ION && c->p.sim_type != YK_SIM_ION_MIXTURE) return 1;
     const int want = c->tpt_req != 0 ? c->tpt_req : ((mixed && c->n >= TPT2_AUTO_MIN_N) ? 2 : 1);
     if (want != 2) return 1;
     return (mixed ? c->fa.lo : c->fa.img_k) ? 2 : 1;
@@ -682,8 +689,9 @@ static int launch_force_t(yk_ctx* c)
         k_force_near<SIM, PREC, MEAS><<<std::min(grid, njobs), PB, 0, c->stream>>>(
             c->pos, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
     } else if (c->pj_tt == 2) {
-        // two targets per thread: ion boxes with fa.lo (mixed) or fa.img_k (FP64) only (pair_tt)
-        if constexpr (SIM != SIM_NUCLEON) {
+        // two targets per thread: ion boxes with fa.lo (mixed) or fa.img_k (FP64), nucleon boxes with
+        // fa.hilo (mixed) only (pair_tt)
+        if constexpr (SIM != SIM_NUCLEON || PREC == PREC_MIXED) {
             if (pairs_tile_boxes<SIM, PREC, PREC == PREC_MIXED>()) {
                 k_tile_boxes<<<c->pj.M, PB, 0, c->stream>>>(c->posf, c->n, c->fa, c->tbox);
                 ++k;

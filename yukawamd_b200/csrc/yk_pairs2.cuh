@@ -1,4 +1,4 @@
-// yk_pairs2.cuh -- the half-pair ion kernels with two targets per thread.
+// yk_pairs2.cuh -- the half-pair kernels with two targets per thread.
 //
 // k_force_pairs2 is k_force_pairs (yk_pairs.cuh) with the target block
 // doubled: a job's targets are the 2 x 128 slots of blocks R and R + 1
@@ -19,12 +19,13 @@
 //   pair (i, j)        : counts iff slot j > slot i, which only tiles R and
 //                        R + 1 need to test.
 //
-// Ions only, on the two paths the ion benchmark boxes take: the FP64 form
-// when the screen's image integers are exact (fa.img_k; the exact
-// comparisons are not compiled in), the mixed form with the hi/lo FP32
-// displacement (fa.lo).  The arithmetic per pair is that of pair_group /
-// pair_group_lo; only the reaction sums (two pairs per lane before the
-// reduction) and the order of the target-side sums differ.
+// Three paths: ions in the FP64 form when the screen's image integers are
+// exact (fa.img_k; the exact comparisons are not compiled in), ions in the
+// mixed form with the hi/lo FP32 displacement (fa.lo), and nucleons in the
+// mixed form with the hi/lo displacement and the flagged exact image near
+// L/2 (fa.hilo).  The arithmetic per pair is that of pair_group,
+// pair_group_lo and pair_group_nn_lo; only the reaction sums (two pairs per
+// lane before the reduction) and the order of the target-side sums differ.
 #pragma once
 
 #include "yk_pairs.cuh"
@@ -34,7 +35,8 @@ namespace yk {
 constexpr int PB2 = 2 * PB;      // target slots of a job
 
 // Bounding box of a warp's 64 targets (two per lane).
-__device__ __forceinline__ WarpBox warp_box2(const ForceArgs& fa, const double4 (&pi)[2], const bool (&act)[2])
+__device__ __forceinline__ WarpBox warp_box2(const ForceArgs& fa, const double4 (&pi)[2], const bool (&act)[2],
+                                             bool proton)
 {
     const float inf = __int_as_float(0x7f800000);
     float lo[3], hi[3];
@@ -45,7 +47,7 @@ __device__ __forceinline__ WarpBox warp_box2(const ForceArgs& fa, const double4 
         lo[k] = fminf(act[0] ? v0 : inf, act[1] ? v1 : inf);
         hi[k] = fmaxf(act[0] ? v0 : -inf, act[1] ? v1 : -inf);
     }
-    return warp_box_of(fa, lo, hi, act[0] || act[1], false);
+    return warp_box_of(fa, lo, hi, act[0] || act[1], proton);
 }
 
 __device__ __forceinline__ float2 lds2(const float* p)
@@ -207,6 +209,171 @@ __device__ __forceinline__ void pair_group_lo2(const ForceArgs& fa, const Screen
     }
 }
 
+// pair_group_nn_lo for two targets per lane (mixed form, nucleons, fa.hilo).
+// The source's hi and lo parts are read once; per target the hi/lo
+// displacement with the screen's image (screen_d_flag_x2's arithmetic), and
+// the pairs flagged near |d| = L/2 take the reference's conditional minimum
+// image on the FP64 positions (int_nn.f:190-195; the target's own position is
+// read again from pos, the source's from gsrc).  Then the HPP terms inside
+// rncut and the p-p Coulomb inside rccut (int_nn.f:208-229) for each target
+// set that a lane of the warp needs.
+template <bool MEAS, bool CHECK>
+__device__ __forceinline__ void pair_group_nn_lo2(const ForceArgs& fa, const ScreenI (&si)[2],
+                                                  const float (&nli)[2][3], const double4* __restrict__ pos,
+                                                  const int (&ii)[2], const float* tlf, const float* tll,
+                                                  const double4* __restrict__ gsrc, int j0, int jlim,
+                                                  const int (&dl)[2], const bool (&act)[2], int sw,
+                                                  TargetAcc<PREC_MIXED, MEAS> (&acc)[2], float* my_acc)
+{
+    const int g = j0 >> 2;
+    const int oa = 8 * g + 2 * sw, ob = 8 * g + 2 * (sw ^ 2);
+    float2 xa[3], xb[3], la[3], lb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        xa[c] = lds2(tlf + c * 2 * SHADOW_TILE + oa);
+        xb[c] = lds2(tlf + c * 2 * SHADOW_TILE + ob);
+        la[c] = lds2(tll + c * 2 * SHADOW_TILE + oa);
+        lb[c] = lds2(tll + c * 2 * SHADOW_TILE + ob);
+    }
+    const float* tw = tlf + 6 * SHADOW_TILE + j0;
+    const float wj[4] = {tw[sw], tw[sw ^ 1], tw[sw ^ 2], tw[sw ^ 3]};
+    const float2 MAG = dup2(12582912.0f), NMAG = dup2(-12582912.0f);
+    float2 da[2][3], db[2][3], ra[2], rb[2];
+    unsigned mn[2], mc[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const float ni[3] = {si[u].nx, si[u].ny, si[u].nz};
+        unsigned fa_ = 0, fb_ = 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float2 dca = __fadd2_rn(xa[c], dup2(ni[c]));
+            const float2 dcb = __fadd2_rn(xb[c], dup2(ni[c]));
+            const float2 ka = __fadd2_rn(__ffma2_rn(dca, dup2(fa.invLf[c]), MAG), NMAG);
+            const float2 kb = __fadd2_rn(__ffma2_rn(dcb, dup2(fa.invLf[c]), MAG), NMAG);
+            const float2 d1a = __ffma2_rn(dup2(-fa.Lh[c]), ka, dca);         // exact
+            const float2 d1b = __ffma2_rn(dup2(-fa.Lh[c]), kb, dcb);
+            fa_ |= (fabsf(d1a.x) >= fa.hLm[c] ? 1u : 0u) | (fabsf(d1a.y) >= fa.hLm[c] ? 2u : 0u);
+            fb_ |= (fabsf(d1b.x) >= fa.hLm[c] ? 1u : 0u) | (fabsf(d1b.y) >= fa.hLm[c] ? 2u : 0u);
+            float2 ea = __fadd2_rn(la[c], dup2(nli[u][c]));
+            float2 eb = __fadd2_rn(lb[c], dup2(nli[u][c]));
+            ea = __ffma2_rn(dup2(-fa.Ll[c]), ka, ea);
+            eb = __ffma2_rn(dup2(-fa.Ll[c]), kb, eb);
+            da[u][c] = __fadd2_rn(d1a, ea);
+            db[u][c] = __fadd2_rn(d1b, eb);
+        }
+        ra[u] = r2_x2(da[u]);
+        rb[u] = r2_x2(db[u]);
+        const unsigned ok = CHECK ? valid4(j0, sw, jlim, dl[u], act[u]) : 0xfu;
+        const unsigned fl = (fa_ | (fb_ << 2)) & ok;
+        if (__any_sync(0xffffffffu, fl != 0)) {
+            // d = x_j - x_i from the reference's d = x_i - x_j and its image
+            const double4 pi = pos[ii[u]];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                if ((fl >> jj) & 1u) {
+                    const double4 pj = gsrc[j0 + (jj ^ sw)];
+                    const float ex = -__double2float_rn(min_image(__dsub_rn(pi.x, pj.x), fa.xl[0], fa.hlb[0]));
+                    const float ey = -__double2float_rn(min_image(__dsub_rn(pi.y, pj.y), fa.xl[1], fa.hlb[1]));
+                    const float ez = -__double2float_rn(min_image(__dsub_rn(pi.z, pj.z), fa.xl[2], fa.hlb[2]));
+                    const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                    float2(&dd)[3] = jj < 2 ? da[u] : db[u];
+                    float2& rr = jj < 2 ? ra[u] : rb[u];
+                    if (jj & 1) {
+                        dd[0].y = ex;
+                        dd[1].y = ey;
+                        dd[2].y = ez;
+                        rr.y = r2;
+                    } else {
+                        dd[0].x = ex;
+                        dd[1].x = ey;
+                        dd[2].x = ez;
+                        rr.x = r2;
+                    }
+                }
+            }
+        }
+        const float r2v[4] = {ra[u].x, ra[u].y, rb[u].x, rb[u].y};
+        const bool ip = si[u].w == 1.0f;
+        mn[u] = 0;
+        mc[u] = 0;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const bool in = (ok >> jj) & 1u;
+            if (in && fa.nuclear_on && r2v[jj] <= fa.rn2f) mn[u] |= 1u << jj;
+            if (in && fa.coulomb_on && ip && wj[jj] == 1.0f && r2v[jj] <= fa.rc2f) mc[u] |= 1u << jj;
+        }
+    }
+    const bool any0 = __any_sync(0xffffffffu, (mn[0] | mc[0]) != 0);
+    const bool any1 = __any_sync(0xffffffffu, (mn[1] | mc[1]) != 0);
+    if (!any0 && !any1) return;
+    float2 fxa[2][3], fxb[2][3];
+    // the terms of target u's four pairs into acc[u]; its reaction products
+    // (fs d, int_nn.f:230-240) into fxa[u], fxb[u]
+    auto terms = [&](int u) {
+        const bool any_n = __any_sync(0xffffffffu, mn[u] != 0);
+        const bool any_c = __any_sync(0xffffffffu, mc[u] != 0);
+        float2 fsa = make_float2(0.f, 0.f), fsb = fsa, ua = fsa, ub = fsa, wa = fsa, wb = fsa;
+        if (any_n) {
+            const float2 Ba = make_float2(wj[0] == si[u].w ? fa.bpcf : fa.bmcf, wj[1] == si[u].w ? fa.bpcf : fa.bmcf);
+            const float2 Bb = make_float2(wj[2] == si[u].w ? fa.bpcf : fa.bmcf, wj[3] == si[u].w ? fa.bpcf : fa.bmcf);
+            nuclear_terms_x2<MEAS>(fa, ra[u], make_float2((mn[u] & 1u) ? 1.f : 0.f, (mn[u] & 2u) ? 1.f : 0.f), Ba,
+                                   fsa, ua, wa);
+            nuclear_terms_x2<MEAS>(fa, rb[u], make_float2((mn[u] & 4u) ? 1.f : 0.f, (mn[u] & 8u) ? 1.f : 0.f), Bb,
+                                   fsb, ub, wb);
+        }
+        if (any_c) {
+            coulomb_terms_x2<MEAS>(fa, ra[u], make_float2((mc[u] & 1u) ? 1.f : 0.f, (mc[u] & 2u) ? 1.f : 0.f), fsa,
+                                   ua, wa);
+            coulomb_terms_x2<MEAS>(fa, rb[u], make_float2((mc[u] & 4u) ? 1.f : 0.f, (mc[u] & 8u) ? 1.f : 0.f), fsb,
+                                   ub, wb);
+        }
+        GroupSum<PREC_MIXED, MEAS> gs;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            fxa[u][c] = __fmul2_rn(fsa, da[u][c]);
+            fxb[u][c] = __fmul2_rn(fsb, db[u][c]);
+            const float2 sc = __fadd2_rn(fxa[u][c], fxb[u][c]);
+            gs.f[c] = -(sc.x + sc.y);
+        }
+        if constexpr (MEAS) {
+            const float2 su = __fadd2_rn(ua, ub);
+            const float2 sv = __fadd2_rn(wa, wb);
+            gs.s[0] = su.x + su.y;
+            gs.s[1] = sv.x + sv.y;
+            const int P[6] = {0, 0, 0, 1, 1, 2}, Q[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const float2 sp = __ffma2_rn(db[u][P[k]], fxb[u][Q[k]], __fmul2_rn(da[u][P[k]], fxa[u][Q[k]]));
+                gs.s[2 + k] = sp.x + sp.y;
+            }
+        }
+        acc[u].add_group2(gs);
+    };
+    // a target set without a pair in the group (for every lane) is skipped
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fxa[u][c] = fxb[u][c] = make_float2(0.f, 0.f);
+    }
+    if (any0) terms(0);
+    if (any1) terms(1);
+    float2 ra3[3], rb3[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        ra3[c] = __fadd2_rn(fxa[0][c], fxa[1][c]);
+        rb3[c] = __fadd2_rn(fxb[0][c], fxb[1][c]);
+    }
+    float t[3];
+    reduce_scatter4_x2(ra3, rb3, t);
+    const int lane = threadIdx.x & 31;
+    const int jl = j0 + sw;
+    if ((lane & 7) == 0 && (!CHECK || jl < jlim)) {
+        my_acc[3 * jl] = t[0];
+        my_acc[3 * jl + 1] = t[1];
+        my_acc[3 * jl + 2] = t[2];
+    }
+}
+
 // pair_group for two targets per lane (FP64 form, ions, fa.img_k).  The
 // FP32 screen reads the source's hi parts once; each selected pair's FP64
 // source position is read once for both targets.  TILEIMG: the tile's image
@@ -306,7 +473,9 @@ __device__ __forceinline__ bool pairs_job2(PairSmem<row_t<PREC>>& sm, const Forc
                                            int C0, int C1, int sg, double* __restrict__ sm_row,
                                            unsigned* __restrict__ err, unsigned& q)
 {
-    static_assert(SIM == SIM_PURE || SIM == SIM_MIX, "two targets per thread: ions only");
+    static_assert(SIM == SIM_PURE || SIM == SIM_MIX || PREC == PREC_MIXED,
+                  "two targets per thread: ions, or nucleons in the mixed form");
+    constexpr bool ION = SIM == SIM_PURE || SIM == SIM_MIX;
     constexpr bool LO = PREC == PREC_MIXED;
     using R_t = real_t<PREC>;
     const int tid = threadIdx.x;
@@ -318,11 +487,13 @@ __device__ __forceinline__ bool pairs_job2(PairSmem<row_t<PREC>>& sm, const Forc
     ScreenI si[2];
     R_t wi[2];
     float nli[2][3];
+    int ii[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         s[u] = 64 * warp + 32 * u + lane;
         const int i = R * PB + s[u];
         act[u] = i < n;
+        ii[u] = act[u] ? i : 0;
         pi[u] = act[u] ? bx.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
         si[u] = load_screen_i(bx.posf, act[u] ? i : 0);
         wi[u] = (SIM == SIM_MIX) ? (R_t)pi[u].w : (R_t)1;
@@ -331,7 +502,7 @@ __device__ __forceinline__ bool pairs_job2(PairSmem<row_t<PREC>>& sm, const Forc
     }
     const bool all_active = (R + 2) * PB <= n;
     const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
-    const WarpBox box = warp_box2(fa, pi, act);
+    const WarpBox box = warp_box2(fa, pi, act, !ION && ((act[0] && pi[0].w == 1.0) || (act[1] && pi[1].w == 1.0)));
     TargetAcc<PREC, MEAS> acc[2];
     acc[0].zero();
     acc[1].zero();
@@ -356,7 +527,29 @@ __device__ __forceinline__ bool pairs_job2(PairSmem<row_t<PREC>>& sm, const Forc
         row_t<PREC>* my_acc = sm.acc_j[st][warp];
         bool used = false;
         const bool reach = box.any && jmin < jlim && (!tb || tile_reaches<SIM>(fa, box, sm.tb[st]));
-        if (reach) {
+        if constexpr (!ION) {
+            if (reach) {
+                unsigned gm = near_groups<SIM>(fa, box, tlf, jlim, jmin);
+                used = gm != 0;
+                if (used) {
+#pragma unroll
+                    for (int k = lane; k < PB * 3; k += 32) my_acc[k] = (row_t<PREC>)0;
+                    __syncwarp();
+                }
+                const float* tll = reinterpret_cast<const float*>(tl);
+                const double4* gsrc = bx.pos + (size_t)C * PB;
+                if (full) {
+                    for (; gm; gm &= gm - 1)
+                        pair_group_nn_lo2<MEAS, false>(fa, si, nli, bx.pos, ii, tlf, tll, gsrc, 4 * (__ffs(gm) - 1),
+                                                       jlim, dl, act, sw, acc, my_acc);
+                } else {
+                    for (; gm; gm &= gm - 1)
+                        pair_group_nn_lo2<MEAS, true>(fa, si, nli, bx.pos, ii, tlf, tll, gsrc, 4 * (__ffs(gm) - 1),
+                                                      jlim, dl, act, sw, acc, my_acc);
+                }
+            }
+        }
+        if (ION && reach) {
             int kcode = -1;
             unsigned gm = near_groups_img(fa, box, tlf, jlim, jmin, kcode);
             used = gm != 0;
