@@ -336,6 +336,27 @@ def read_traffic(kind, precision):
     return None
 
 
+def read_pipe(kind, precision):
+    """Busy share of the bounding pipe of the force kernel in one ncu capture
+    (a line "pipe_pct_per_launch <kind> <precision>: <pct> <pipe>" in the
+    committed ncu summaries), as {"pipe", "pct"}; None if absent."""
+    key = "pipe_pct_per_launch %s %s:" % (kind, precision)
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for name in sorted(os.listdir(pdir)):
+        if not name.endswith(".md"):
+            continue
+        for line in open(os.path.join(pdir, name)):
+            if line.startswith(key):
+                f = line.split(":", 1)[1].split()
+                try:
+                    return {"pipe": f[1], "pct": float(f[0]), "source": "profiles/" + name}
+                except (ValueError, IndexError):
+                    return None
+    return None
+
+
 def _pairs_of_rows(n, r0, r1):
     """Unique pairs of target rows r0 <= i < r1 (row i pairs with j > i)."""
     r1 = min(r1, n - 1)
@@ -430,7 +451,10 @@ def run_ours(args, dist):
                           % (e.kernel_name, force_ms, perf.force_calls),
                 "peak_source": "measured live by yk_peak_probe (%s FMA chain, all SMs)"
                                % ("FP64" if prec_kind == 0 else "FP32"),
-                "flops_per_pair": fpp, "force_share_of_step": perf.force_ms / perf.run_ms}
+                "flops_per_pair": fpp, "force_share_of_step": perf.force_ms / perf.run_ms,
+                "pipe_ncu": read_pipe(kind, args.precision),
+                "note": "achieved counts flops_per_pair on every unique pair; the pipe_ncu busy share "
+                        "is what the hardware pipe did"}
 
     out = {"metric": BASELINE_METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
            "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
@@ -480,7 +504,7 @@ def run_ours(args, dist):
                                             % (e2.kernel_name, fms2, perf2.force_calls),
                                   "peak_source": "measured live by yk_peak_probe (%s FMA chain, all SMs)"
                                                  % ("FP32" if kind2 else "FP64"),
-                                  "flops_per_pair": fpp}
+                                  "flops_per_pair": fpp, "pipe_ncu": read_pipe(kind, other)}
         e2.close()
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
             out["mixed"]["vs_oracle"] = mixed_vs_oracle(w)
