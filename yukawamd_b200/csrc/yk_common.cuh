@@ -231,21 +231,6 @@ __device__ __forceinline__ float2 sub2(float2 x, float2 y)
     return __ffma2_rn(y, make_float2(-1.f, -1.f), x);
 }
 
-// exp_neg_f32_xu on two values, the FP32 arithmetic paired.
-__device__ __forceinline__ float2 exp_neg_f32_xu_x2(float2 t)
-{
-    const float L2E_HI = 1.44269502162933349609375f;
-    const float L2E_LO_LN2 = 1.3349758e-8f;
-    const float LN2 = 0.693147180559945309f;
-    const float2 nl = make_float2(-L2E_HI, -L2E_HI);
-    const float2 yh = __fmul2_rn(t, nl);
-    const float2 e1 = __ffma2_rn(t, nl, make_float2(-yh.x, -yh.y));
-    const float2 c = __ffma2_rn(e1, make_float2(LN2, LN2),
-                                __fmul2_rn(t, make_float2(-L2E_LO_LN2, -L2E_LO_LN2)));
-    const float2 r = make_float2(ex2_approx(yh.x), ex2_approx(yh.y));
-    return __ffma2_rn(r, c, r);
-}
-
 // Two compensated sums (cf32::add) advanced together.
 __device__ __forceinline__ void cf32_add2(cf32& a, cf32& b, float2 x)
 {

@@ -608,11 +608,24 @@ __device__ __forceinline__ void ion_terms_x2(const ForceArgs& fa, float2 r2, flo
 //            fn = (2 aa e + B) e / Lambda, u = (aa e + B) e, w = fn r^2
 //   p-p Coulomb: fc = vc (1 + mu r) e^{-mu r} / r^3, u = vc e^{-mu r}/r - evcut
 //            (evcut includes vc for nucleons), w = fc r^2
+// Both exponentials are the hardware base-2 exponential of the rounded
+// product y = -t log2(e), as in ion_terms_x2: the rounding of y changes the
+// result by at most |y| 2^-24 ln 2 relative, about the instruction's own
+// error (2 ulp) where the terms carry the force (nuclear r^2 / 2 Lambda and
+// Coulomb mu r of a few) and below 1e-6 where they are weighted by e^-10 or
+// less; 1/r is the hardware reciprocal-root estimate.
+__device__ __forceinline__ float2 exp_neg_x2(float2 t)
+{
+    const float L2E = 1.44269502162933349609375f;           // float(log2 e)
+    const float2 y = __fmul2_rn(t, make_float2(-L2E, -L2E));
+    return make_float2(ex2_approx(y.x), ex2_approx(y.y));
+}
+
 template <bool MEAS>
 __device__ __forceinline__ void nuclear_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2 B, float2& fs,
                                                  float2& u, float2& w)
 {
-    const float2 e = exp_neg_f32_xu_x2(__fmul2_rn(r2, make_float2(fa.xp2if, fa.xp2if)));
+    const float2 e = exp_neg_x2(__fmul2_rn(r2, make_float2(fa.xp2if, fa.xp2if)));
     const float2 em = __fmul2_rn(e, msk);
     const float2 fn = __fmul2_rn(make_float2(fa.xpif, fa.xpif),
                                  __fmul2_rn(__ffma2_rn(make_float2(fa.aa2f, fa.aa2f), e, B), em));
@@ -628,11 +641,12 @@ __device__ __forceinline__ void coulomb_terms_x2(const ForceArgs& fa, float2 r2,
                                                  float2& w)
 {
     const float2 r2s = make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f);
-    const float2 rinv = make_float2(rsqrt_f32(r2s.x), rsqrt_f32(r2s.y));
+    const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
     const float2 mr = __fmul2_rn(make_float2(fa.xmucf, fa.xmucf), __fmul2_rn(r2s, rinv));
-    const float2 er = __fmul2_rn(__fmul2_rn(exp_neg_f32_xu_x2(mr), rinv), make_float2(fa.vcf, fa.vcf));
-    const float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(make_float2(1.0f, 1.0f), mr), er), __fmul2_rn(rinv, rinv));
-    const float2 fc = __fmul2_rn(f, msk);
+    const float2 er = __fmul2_rn(__fmul2_rn(exp_neg_x2(mr), rinv), make_float2(fa.vcf, fa.vcf));
+    // fc = (1 + mu r) q with q = er / r^2, masked
+    const float2 q = __fmul2_rn(er, __fmul2_rn(__fmul2_rn(rinv, rinv), msk));
+    const float2 fc = __ffma2_rn(mr, q, q);
     fs = __fadd2_rn(fs, fc);
     if constexpr (MEAS) {
         u = __ffma2_rn(__fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf)), msk, u);
