@@ -296,6 +296,20 @@ __device__ __forceinline__ double exp_neg_f64(double t)
     return t > 700.0 ? 0.0 : __hiloint2double(hi, __double2loint(res));
 }
 
+// FP64 1/sqrt(x) for x > 0 inside the FP32 normal range (a pair's r^2, or 1
+// for a masked pair): Newton's iteration y <- y (3/2 - (x/2) y^2) from the FP32
+// hardware estimate.  Each step squares the relative error (about 2^-22 ->
+// 2^-43 -> below the FP64 rounding), so two steps leave the rounding errors
+// of the steps themselves, a few ulp.
+__device__ __forceinline__ double rsqrt_nr64(double x)
+{
+    double y = (double)rsqrtf(__double2float_rn(x));
+    const double h = 0.5 * x;
+    y = __dmul_rn(y, __fma_rn(-__dmul_rn(h, y), y, 1.5));
+    y = __dmul_rn(y, __fma_rn(-__dmul_rn(h, y), y, 1.5));
+    return y;
+}
+
 // FP32 1/sqrt(x): hardware estimate plus one Newton step.
 __device__ __forceinline__ float rsqrt_f32(float x)
 {

@@ -15,9 +15,10 @@
 //         u = (aa e + B) e, fs = (2 aa e + B) e / Lambda, B = bb +/- cc by
 //         species equality; Coulomb (p-p, r^2 <= rccut^2): vc x the ion terms.
 //
-// PREC_FP64: all FP64 (exp_neg_f64, our table-driven exp, and rsqrt() from
-// the CUDA math library; rsqrt replaces the reference's sqrt and divide,
-// 1/(r r^2) = rinv^3).
+// PREC_FP64: all FP64 (exp_neg_f64, our table-driven exp; for ions
+// rsqrt_nr64, Newton's iteration from the FP32 hardware estimate, for the
+// nucleon Coulomb term the library rsqrt; the reciprocal root replaces the
+// reference's sqrt and divide, 1/(r r^2) = rinv^3).
 // PREC_MIXED: the r^2, rsqrt, exp and force terms in FP32.  Pairs take their
 // displacement from the shadow's hi/lo parts (screen_d_x2: exact FP32 hi-part
 // differences plus a lo correction, no FP64 arithmetic) when the box allows it
@@ -331,7 +332,7 @@ __device__ __forceinline__ void phys64(const ForceArgs& fa, double wi, double wj
     o.hit = false;
     if constexpr (SIM == SIM_PURE || SIM == SIM_MIX) {
         if (valid && r2 <= fa.rc2) {
-            const double rinv = rsqrt(r2);
+            const double rinv = rsqrt_nr64(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;
             const double er = exp_neg_f64(mr) * rinv;                // e^{-mu r}/r
@@ -356,6 +357,9 @@ __device__ __forceinline__ void phys64(const ForceArgs& fa, double wi, double wj
             o.hit = true;
         }
         if (fa.coulomb_on && wi == 1.0 && wj == 1.0 && r2 <= fa.rc2) {
+            // the library root: on this branchy single-pair path the longer
+            // dependency chain of rsqrt_nr64 made the 51,200-nucleon step
+            // 3.5 % slower (the ion paths interleave four pairs and gain 2 %)
             const double rinv = rsqrt(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;
@@ -525,7 +529,7 @@ __device__ __forceinline__ void ion_terms_nb(const ForceArgs& fa, double dx, dou
         const double r2 = o.dx * o.dx + o.dy * o.dy + o.dz * o.dz;
         const bool hit = sel && r2 <= fa.rc2;
         const double r2s = hit ? r2 : 1.0;
-        const double rinv = rsqrt(r2s);
+        const double rinv = rsqrt_nr64(r2s);
         const double r = r2s * rinv;
         const double mr = fa.xmuc * r;
         const double er = exp_neg_f64(mr) * rinv;
