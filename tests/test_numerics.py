@@ -104,7 +104,7 @@ def test_underflow_flushes_to_zero():
 
 def _f64_source_table():
     text = open(SRC).read()
-    body = text[text.index("g_exp2_64[64] = {"):]
+    body = text[text.index("g_exp2_256[256] = {"):]
     body = body[body.index("{") + 1:body.index("};")]
     return [float(v) for v in body.replace("\n", " ").split(",") if v.strip()]
 
@@ -118,19 +118,19 @@ def exp_neg_f64(t):
     import struct
     tab = _f64_source_table()
     MAG = 6755399441055744.0
-    kd = _fma64(-t, 92.33248261689366, MAG)
+    kd = _fma64(-t, 369.3299304675746, MAG)
     nf = kd - MAG
-    r = _fma64(-nf, 3.623510646634843e-19, _fma64(-nf, 0.010830424696249145, -t))
-    q = 1.0 / 120.0
-    for c in (1.0 / 24.0, 1.0 / 6.0, 0.5, 1.0):
+    r = _fma64(-nf, 9.058776616587108e-20, _fma64(-nf, 0.0027076061740622863, -t))
+    q = 1.0 / 24.0
+    for c in (1.0 / 6.0, 0.5, 1.0):
         q = _fma64(q, r, c)
     p = q * r
     bits = struct.unpack("<q", struct.pack("<d", kd))[0]
     ni = ((bits & 0xffffffff) ^ 0x80000000) - 0x80000000      # low word as int32
-    tj = tab[ni & 63]
+    tj = tab[ni & 255]
     res = _fma64(tj, p, tj)
     rb = struct.unpack("<q", struct.pack("<d", res))[0]
-    rb += (ni >> 6) << 52
+    rb += (ni >> 8) << 52
     return 0.0 if t > 700.0 else struct.unpack("<d", struct.pack("<q", rb))[0]
 
 
@@ -139,16 +139,16 @@ def test_f64_table_is_correctly_rounded():
     getcontext().prec = 50
     ln2 = Decimal(2).ln()
     tab = _f64_source_table()
-    assert len(tab) == 64
+    assert len(tab) == 256
     for j, v in enumerate(tab):
-        assert v == float((Decimal(j) / 64 * ln2).exp())
+        assert v == float((Decimal(j) / 256 * ln2).exp())
 
 
 def test_f64_exp_within_three_ulp():
     from decimal import Decimal, getcontext
     getcontext().prec = 50
     rng = np.random.default_rng(11)
-    ts = np.concatenate([[0.0, 1e-300, 1e-9, 0.5, 1.0, np.log(2.0) / 128, 10.0, 53.0, 699.0],
+    ts = np.concatenate([[0.0, 1e-300, 1e-9, 0.5, 1.0, np.log(2.0) / 512, np.log(2.0) / 128, 10.0, 53.0, 699.0],
                          rng.uniform(0.0, 12.0, 300), rng.uniform(0.0, 700.0, 100)])
     worst = 0.0
     for t in ts:

@@ -305,6 +305,7 @@ static void setup_args(yk_ctx* c)
         // coordinate and box length is below SHADOW_EXACT; a margin of 2 leaves
         // room for coordinates up to 2 L.
         f.lo = (f.img_k && 2.0 * Lmax < SHADOW_EXACT) ? 1 : 0;
+        f.exp_ok = (std::isfinite(p.rccut) && p.xmuc >= 0.0 && p.xmuc * std::max(p.rccut, 1.0) <= 690.0) ? 1 : 0;
         f.hilo = (2.0 * Lmax < SHADOW_EXACT) ? 1 : 0;
         for (int k = 0; k < 3; ++k) {
             // the hi-part displacement is exact and within 2^-8 fm of the
@@ -476,7 +477,7 @@ static int pair_tt(const yk_ctx* c)
     if (c->p.sim_type != YK_SIM_PURE_ION && c->p.sim_type != YK_SIM_ION_MIXTURE) return 1;
     const int want = c->tpt_req != 0 ? c->tpt_req : ((mixed && c->n >= TPT2_AUTO_MIN_N) ? 2 : 1);
     if (want != 2) return 1;
-    return (mixed ? c->fa.lo : c->fa.img_k) ? 2 : 1;
+    return (mixed ? c->fa.lo : (c->fa.img_k && c->fa.exp_ok)) ? 2 : 1;
 }
 
 static int auto_pair_seg(const yk_ctx* c)
@@ -689,7 +690,7 @@ static int launch_force_t(yk_ctx* c)
         k_force_near<SIM, PREC, MEAS><<<std::min(grid, njobs), PB, 0, c->stream>>>(
             c->pos, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
     } else if (c->pj_tt == 2) {
-        // two targets per thread: ion boxes with fa.lo (mixed) or fa.img_k (FP64), nucleon boxes with
+        // two targets per thread: ion boxes with fa.lo (mixed) or fa.img_k and fa.exp_ok (FP64), nucleon boxes with
         // fa.hilo (mixed) only (pair_tt)
         if constexpr (SIM != SIM_NUCLEON || PREC == PREC_MIXED) {
             if (pairs_tile_boxes<SIM, PREC, PREC == PREC_MIXED>()) {
@@ -715,7 +716,7 @@ static int launch_force_t(yk_ctx* c)
                 k_force_pairs<SIM, PREC, MEAS, true><<<std::min(grid, njobs), PB, 0, c->stream>>>(
                     c->pos, c->posf, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
             }
-        } else if (SIM != SIM_NUCLEON && c->fa.img_k) {
+        } else if (SIM != SIM_NUCLEON && c->fa.img_k && c->fa.exp_ok) {
             if constexpr (SIM != SIM_NUCLEON) {
                 const int grid = persistent_grid<k_force_pairs<SIM, PREC, MEAS, false, true>>(c->dev);
                 k_force_pairs<SIM, PREC, MEAS, false, true><<<std::min(grid, njobs), PB, 0, c->stream>>>(

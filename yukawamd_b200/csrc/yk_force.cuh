@@ -65,6 +65,8 @@ struct ForceArgs {
     float scr_c2, scr_n2;
     int n, nuclear_on, coulomb_on, mix_compat;
     int img_k;                       // the screen's image integers are exact (see setup)
+    int exp_ok;                      // mu max(r_c, 1) <= 690: every exponent of an ion pair
+                                     // (masked pairs take r = 1) is inside exp_neg_f64's range
     // mixed form, ions: the displacement from the hi/lo shadow parts
     // (screen_d_x2); Lh = box on the SHADOW_Q grid, Ll = box - Lh
     float Lh[3], Ll[3];
@@ -492,7 +494,7 @@ __device__ __forceinline__ float2 screen_r2_tile_x2(const float2 (&th)[3], const
     return __ffma2_rn(d[0], d[0], r2);
 }
 
-template <int PREC, bool MEAS>
+template <int PREC, bool MEAS, bool RANGE = true>
 __device__ __forceinline__ void ion_terms_nb(const ForceArgs& fa, double dx, double dy, double dz, bool sel,
                                              PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o);
 
@@ -503,7 +505,10 @@ template <int PREC, bool MEAS>
 __device__ __forceinline__ void ion_pair_tile(const ForceArgs& fa, const double4& pit, const double4& pj, bool sel,
                                               PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o)
 {
-    ion_terms_nb<PREC, MEAS>(fa, __dsub_rn(pit.x, pj.x), __dsub_rn(pit.y, pj.y), __dsub_rn(pit.z, pj.z), sel, o);
+    // only the exact-image kernels take the tile image, and those run only on
+    // boxes with fa.exp_ok
+    ion_terms_nb<PREC, MEAS, false>(fa, __dsub_rn(pit.x, pj.x), __dsub_rn(pit.y, pj.y), __dsub_rn(pit.z, pj.z),
+                                    sel, o);
 }
 
 template <int PREC, bool MEAS, bool IMGK = false>
@@ -514,11 +519,11 @@ __device__ __forceinline__ void ion_pair_nb(const ForceArgs& fa, const double4& 
     const double dx = image_k<IMGK>(fa, __dsub_rn(pi.x, pj.x), k[0], 0);
     const double dy = image_k<IMGK>(fa, __dsub_rn(pi.y, pj.y), k[1], 1);
     const double dz = image_k<IMGK>(fa, __dsub_rn(pi.z, pj.z), k[2], 2);
-    ion_terms_nb<PREC, MEAS>(fa, dx, dy, dz, sel, o);
+    ion_terms_nb<PREC, MEAS, !IMGK>(fa, dx, dy, dz, sel, o);       // IMGK kernels run with fa.exp_ok
 }
 
 // The pair terms of ion_pair_nb from the minimum-image displacement.
-template <int PREC, bool MEAS>
+template <int PREC, bool MEAS, bool RANGE>
 __device__ __forceinline__ void ion_terms_nb(const ForceArgs& fa, double dx, double dy, double dz, bool sel,
                                              PairOut<std::conditional_t<PREC == PREC_FP64, double, float>>& o)
 {
@@ -532,7 +537,7 @@ __device__ __forceinline__ void ion_terms_nb(const ForceArgs& fa, double dx, dou
         const double rinv = rsqrt_nr64(r2s);
         const double r = r2s * rinv;
         const double mr = fa.xmuc * r;
-        const double er = exp_neg_f64(mr) * rinv;
+        const double er = exp_neg_f64<RANGE>(mr) * rinv;
         const double fs = (1.0 + mr) * er * (rinv * rinv);
         o.fs = hit ? fs : 0.0;
         o.u = (MEAS && hit) ? er - fa.evcut : 0.0;
