@@ -791,8 +791,9 @@ static int enqueue_finish(yk_ctx* c, bool meas, int kin_mode, bool series)
 static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool resort, bool timed = false)
 {
     int k = 0;
+    // A repack of positions set on the host is not needed here: the drift
+    // moves them and k_pack_slots packs the moved ones.
     if (resort || c->need_sort) k += enqueue_order(c, true);
-    else if (c->pos_dirty) k += enqueue_order(c, false);
     const int nb = c->nvb;
     const int nb3 = (int)((3LL * c->n + VBLOCK - 1) / VBLOCK);   // element-wise drifts
     cudaStream_t st = c->stream;
@@ -809,6 +810,7 @@ static int enqueue_newton(yk_ctx* c, bool meas, bool series, bool resort, bool t
         break;
     }
     k_pack_slots<<<nb, VBLOCK, 0, st>>>(c->perm, c->x, c->zii, c->pos, c->posf, c->n, s.pack_w);
+    c->pos_dirty = false;
     k += 2;
     k += enqueue_force(c, meas, timed);
     int kin_mode;
@@ -1519,12 +1521,10 @@ int yk_set_state(yk_ctx* c, const double* x, const double* v, const double* vold
     *c->h_err = 0;
     g_launches += k;
     if (bad) return fail(c, YK_ERR_NONFINITE, "NaN or Inf in a state array");
-    if (x) {
-        // keep the current Morton order; the next scheduled sort refreshes it
-        c->pos_dirty = true;
-        g_launches += enqueue_order(c, false);
-        CK(c, cudaStreamSynchronize(c->stream));
-    }
+    // new positions keep the current slot order (the next scheduled sort
+    // refreshes it); the packed copies are rebuilt by the next call that
+    // reads them (a force call) or moves the positions first (a step)
+    if (x) c->pos_dirty = true;
     return YK_OK;
 }
 

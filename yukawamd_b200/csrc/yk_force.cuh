@@ -797,6 +797,12 @@ struct TargetAcc<PREC_MIXED, MEAS> {
             for (int k = 0; k < NSCAL; ++k) sd[k] += (double)g.s[k];
         }
     }
+    // only the force part of a group's sum (the measuring sums kept elsewhere)
+    __device__ __forceinline__ void add_group2_force(const GroupSum<PREC_MIXED, MEAS>& g)
+    {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fd[c] += (double)g.f[c];
+    }
     __device__ __forceinline__ double force(int k) const { return f[k].value() + fd[k]; }
     __device__ __forceinline__ double scal(int k) const
     {

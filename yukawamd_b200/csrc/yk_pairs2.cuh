@@ -86,12 +86,17 @@ __device__ __forceinline__ unsigned valid4(int j0, int sw, int jlim, int dl, boo
 // source's hi and lo parts are read once; per target the displacement is
 // that of disp_tile_x2 (TILEIMG: the tile's image folded into th / tl2) or
 // screen_d_x2 (each pair's own image), the terms those of ion_terms_x2.
+// Measuring: the group's energy, virial and pressure-tensor sums of both
+// targets, weighted by Z_i, go into the lane's FP32 tile sums ms (the job
+// adds them to FP64 sums after each tile); they are sums over all pairs, so
+// no per-target accumulator is needed.
 template <int SIM, bool MEAS, bool CHECK, bool TILEIMG>
 __device__ __forceinline__ void pair_group_lo2(const ForceArgs& fa, const ScreenI (&si)[2], const float (&nli)[2][3],
                                                const float (&th)[2][3], const float (&tl2)[2][3],
                                                const float (&wi)[2], const float* tlf, const float* tll, int j0,
                                                int jlim, const int (&dl)[2], const bool (&act)[2], int sw,
-                                               TargetAcc<PREC_MIXED, MEAS> (&acc)[2], float* my_acc)
+                                               TargetAcc<PREC_MIXED, MEAS> (&acc)[2], float* my_acc,
+                                               float (&ms)[NSCAL])
 {
     const int g = j0 >> 2;
     const int oa = 8 * g + 2 * sw, ob = 8 * g + 2 * (sw ^ 2);
@@ -173,8 +178,10 @@ __device__ __forceinline__ void pair_group_lo2(const ForceArgs& fa, const Screen
                 const float2 sp = __ffma2_rn(db[u][P[k]], fxb[Q[k]], __fmul2_rn(da[u][P[k]], fxa[Q[k]]));
                 gs.s[2 + k] = sp.x + sp.y;
             }
+#pragma unroll
+            for (int k = 0; k < NSCAL; ++k) ms[k] = fmaf(gs.s[k], wi[u], ms[k]);
         }
-        acc[u].add_group2(gs);
+        acc[u].add_group2_force(gs);
         // reaction on j: Z_i fs d (int_ion_mix.f:180), both targets' terms
         // summed in the lane
         const float2 ha = __fmul2_rn(fsa, dup2(wi[u])), hb = __fmul2_rn(fsb, dup2(wi[u]));
@@ -506,6 +513,15 @@ __device__ __forceinline__ bool pairs_job2(PairSmem<row_t<PREC>>& sm, const Forc
     TargetAcc<PREC, MEAS> acc[2];
     acc[0].zero();
     acc[1].zero();
+    // mixed ions, measuring: the lane's Z_i-weighted sums of both targets,
+    // FP32 within a tile (pair_group_lo2), FP64 across tiles
+    float ms[NSCAL];
+    double msd[NSCAL];
+#pragma unroll
+    for (int k = 0; k < NSCAL; ++k) {
+        ms[k] = 0.f;
+        msd[k] = 0.0;
+    }
     const bool tb = TB && bx.tbox != nullptr;
 
     if (tid == 0) {
@@ -584,24 +600,31 @@ __device__ __forceinline__ bool pairs_job2(PairSmem<row_t<PREC>>& sm, const Forc
                         for (; gm; gm &= gm - 1)
                             pair_group_lo2<SIM, MEAS, false, true>(fa, si, nli, th, tl2, wf, tlf, tll,
                                                                    4 * (__ffs(gm) - 1), jlim, dl, act, sw, acc,
-                                                                   my_acc);
+                                                                   my_acc, ms);
                     } else {
                         for (; gm; gm &= gm - 1)
                             pair_group_lo2<SIM, MEAS, true, true>(fa, si, nli, th, tl2, wf, tlf, tll,
                                                                   4 * (__ffs(gm) - 1), jlim, dl, act, sw, acc,
-                                                                  my_acc);
+                                                                  my_acc, ms);
                     }
                 } else {
                     if (full) {
                         for (; gm; gm &= gm - 1)
                             pair_group_lo2<SIM, MEAS, false, false>(fa, si, nli, th, tl2, wf, tlf, tll,
                                                                     4 * (__ffs(gm) - 1), jlim, dl, act, sw, acc,
-                                                                    my_acc);
+                                                                    my_acc, ms);
                     } else {
                         for (; gm; gm &= gm - 1)
                             pair_group_lo2<SIM, MEAS, true, false>(fa, si, nli, th, tl2, wf, tlf, tll,
                                                                    4 * (__ffs(gm) - 1), jlim, dl, act, sw, acc,
-                                                                   my_acc);
+                                                                   my_acc, ms);
+                    }
+                }
+                if constexpr (MEAS) {
+#pragma unroll
+                    for (int k = 0; k < NSCAL; ++k) {
+                        msd[k] += (double)ms[k];
+                        ms[k] = 0.f;
                     }
                 }
             } else {
@@ -681,8 +704,11 @@ __device__ __forceinline__ bool pairs_job2(PairSmem<row_t<PREC>>& sm, const Forc
     if constexpr (MEAS) {
         double S[NSCAL];
 #pragma unroll
-        for (int k = 0; k < NSCAL; ++k)
-            S[k] = (act[0] ? acc[0].scal(k) * (double)wi[0] : 0.0) + (act[1] ? acc[1].scal(k) * (double)wi[1] : 0.0);
+        for (int k = 0; k < NSCAL; ++k) {
+            if constexpr (LO && ION) S[k] = msd[k];           // already weighted by Z_i
+            else S[k] = (act[0] ? acc[0].scal(k) * (double)wi[0] : 0.0) +
+                        (act[1] ? acc[1].scal(k) * (double)wi[1] : 0.0);
+        }
         block_sum_store<NSCAL>(S, sm.red, sm_row);
         __syncthreads();
     }
