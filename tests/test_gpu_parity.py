@@ -91,6 +91,21 @@ def test_ragged_sizes(gpu, orc, kind, n, kern):
     check_accel(orc, w, abi.YK_PREC_FP64, False, tuning=KERNELS[kern])
 
 
+@pytest.mark.parametrize("n", [2, 17, 129, 257, 513, 1500, 4000])
+@pytest.mark.parametrize("sort", ["sorted", "unsorted"])
+def test_mixed_nucleons_species_modes(gpu, orc, n, sort):
+    """The mixed nucleon kernel's species modes (neutron warps without the
+    Coulomb term and flag test where the nuclear range is short of L/2;
+    proton warps on proton tiles without species tests; anything else the
+    general path): species-major slot order makes single-species warps and
+    tiles, the identity order mixed ones; small boxes have the nuclear range
+    beyond L/2.  Measuring and force-only calls against the oracle."""
+    w = workload("nn", n, 60 + n)
+    tun = dict(force_kernel=abi.KERNEL_PAIRS, sort_every=50 if sort == "sorted" else -1)
+    check_accel(orc, w, abi.YK_PREC_MIXED, True, tuning=tun)
+    check_accel(orc, w, abi.YK_PREC_MIXED, False, tuning=tun)
+
+
 @pytest.mark.parametrize("kern", ["rows", "pairs", "near"])
 @pytest.mark.parametrize("mode", [abi.YK_MIX_COMPAT, abi.YK_MIX_FIXED], ids=["compat", "fixed"])
 def test_mix_last_particle_mode(gpu, orc, mode, kern):

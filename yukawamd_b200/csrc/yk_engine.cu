@@ -307,6 +307,8 @@ static void setup_args(yk_ctx* c)
         f.lo = (f.img_k && 2.0 * Lmax < SHADOW_EXACT) ? 1 : 0;
         f.exp_ok = (std::isfinite(p.rccut) && p.xmuc >= 0.0 && p.xmuc * std::max(p.rccut, 1.0) <= 690.0) ? 1 : 0;
         f.hilo = (2.0 * Lmax < SHADOW_EXACT) ? 1 : 0;
+        f.nn_short = (f.scr_n2 < 0.0f ||
+                      std::sqrt((double)f.scr_n2) + std::ldexp(1.0, -5) < 0.5 * Lmin) ? 1 : 0;
         for (int k = 0; k < 3; ++k) {
             // the hi-part displacement is exact and within 2^-8 fm of the
             // reference's FP64 one, so |d| < L/2 - 2^-7 leaves the image

@@ -65,6 +65,9 @@ struct ForceArgs {
     float scr_c2, scr_n2;
     int n, nuclear_on, coulomb_on, mix_compat;
     int img_k;                       // the screen's image integers are exact (see setup)
+    int nn_short;                    // nucleons: the nuclear screening radius is below L/2 - 2^-5 fm
+                                     // on every axis (or the nuclear term is off), so a pair near
+                                     // |d| = L/2 on some axis is out of nuclear range in either image
     int exp_ok;                      // mu max(r_c, 1) <= 690: every exponent of an ion pair
                                      // (masked pairs take r = 1) is inside exp_neg_f64's range
     // mixed form, ions: the displacement from the hi/lo shadow parts

@@ -395,7 +395,18 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
 // pair gets the reference's image.  Then the HPP terms inside rncut and the
 // p-p Coulomb inside rccut (int_nn.f:208-229), two pairs per FP32x2
 // instruction, a branch per term only when no lane of the warp needs it.
-template <bool MEAS, bool CHECK>
+// MODE (warp-uniform, from the species of the warp's targets and the tile's
+// sources; slots are in species-major order, so nearly every warp and tile
+// holds one species):
+//   NN_ANY  any species;
+//   NN_NOP  no proton target (and fa.nn_short): no Coulomb term, and no flag
+//           test, since a pair near |d| = L/2 is beyond the nuclear range
+//           under either image;
+//   NN_PP   proton targets and proton sources only: every pair is a like pair
+//           and takes the Coulomb term, no species tests.
+constexpr int NN_ANY = 0, NN_NOP = 1, NN_PP = 2;
+
+template <bool MEAS, bool CHECK, int MODE = NN_ANY>
 __device__ __forceinline__ void pair_group_nn_lo(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
                                                  const double4& pi, const float* tlf, const float* tll,
                                                  const double4* __restrict__ gsrc, int j0, int jlim, bool diag,
@@ -405,8 +416,14 @@ __device__ __forceinline__ void pair_group_nn_lo(const ForceArgs& fa, const Scre
     const int g = j0 >> 2;
     float2 da[3], db[3];
     unsigned fla = 0, flb = 0;
-    float2 ra = screen_d_flag_x2(fa, si, nli, tlf, tll, g, 2 * sw, da, fla);
-    float2 rb = screen_d_flag_x2(fa, si, nli, tlf, tll, g, 2 * (sw ^ 2), db, flb);
+    float2 ra, rb;
+    if constexpr (MODE == NN_NOP) {
+        ra = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * sw, da);
+        rb = screen_d_x2(fa, si, nli, tlf, tll, g, 2 * (sw ^ 2), db);
+    } else {
+        ra = screen_d_flag_x2(fa, si, nli, tlf, tll, g, 2 * sw, da, fla);
+        rb = screen_d_flag_x2(fa, si, nli, tlf, tll, g, 2 * (sw ^ 2), db, flb);
+    }
     unsigned ok = 0xfu;
     if constexpr (CHECK) {
         ok = 0;
@@ -417,7 +434,7 @@ __device__ __forceinline__ void pair_group_nn_lo(const ForceArgs& fa, const Scre
         }
     }
     const unsigned fl = (fla | (flb << 2)) & ok;
-    if (__any_sync(0xffffffffu, fl != 0)) {
+    if (MODE != NN_NOP && __any_sync(0xffffffffu, fl != 0)) {
         // d = x_j - x_i from the reference's d = x_i - x_j and its image
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
@@ -444,23 +461,30 @@ __device__ __forceinline__ void pair_group_nn_lo(const ForceArgs& fa, const Scre
         }
     }
     const float* tw = tlf + 6 * SHADOW_TILE + j0;
-    const float wj[4] = {tw[sw], tw[sw ^ 1], tw[sw ^ 2], tw[sw ^ 3]};
+    float wj[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) wj[jj] = MODE == NN_PP ? 1.0f : tw[jj ^ sw];
     const float r2v[4] = {ra.x, ra.y, rb.x, rb.y};
-    const bool ip = si.w == 1.0f;
+    const bool ip = MODE == NN_PP || si.w == 1.0f;
     unsigned mn = 0, mc = 0;
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) {
         const bool in = (ok >> jj) & 1u;
         if (in && fa.nuclear_on && r2v[jj] <= fa.rn2f) mn |= 1u << jj;
-        if (in && fa.coulomb_on && ip && wj[jj] == 1.0f && r2v[jj] <= fa.rc2f) mc |= 1u << jj;
+        if (MODE != NN_NOP && in && fa.coulomb_on && ip && wj[jj] == 1.0f && r2v[jj] <= fa.rc2f) mc |= 1u << jj;
     }
     const bool any_n = __any_sync(0xffffffffu, mn != 0);
-    const bool any_c = __any_sync(0xffffffffu, mc != 0);
+    const bool any_c = MODE != NN_NOP && __any_sync(0xffffffffu, mc != 0);
     if (!any_n && !any_c) return;
     float2 fsa = make_float2(0.f, 0.f), fsb = fsa, ua = fsa, ub = fsa, wa = fsa, wb = fsa;
     if (any_n) {
-        const float2 Ba = make_float2(wj[0] == si.w ? fa.bpcf : fa.bmcf, wj[1] == si.w ? fa.bpcf : fa.bmcf);
-        const float2 Bb = make_float2(wj[2] == si.w ? fa.bpcf : fa.bmcf, wj[3] == si.w ? fa.bpcf : fa.bmcf);
+        float2 Ba, Bb;
+        if constexpr (MODE == NN_PP) {
+            Ba = Bb = make_float2(fa.bpcf, fa.bpcf);
+        } else {
+            Ba = make_float2(wj[0] == si.w ? fa.bpcf : fa.bmcf, wj[1] == si.w ? fa.bpcf : fa.bmcf);
+            Bb = make_float2(wj[2] == si.w ? fa.bpcf : fa.bmcf, wj[3] == si.w ? fa.bpcf : fa.bmcf);
+        }
         nuclear_terms_x2<MEAS>(fa, ra, make_float2((mn & 1u) ? 1.f : 0.f, (mn & 2u) ? 1.f : 0.f), Ba, fsa, ua, wa);
         nuclear_terms_x2<MEAS>(fa, rb, make_float2((mn & 4u) ? 1.f : 0.f, (mn & 8u) ? 1.f : 0.f), Bb, fsb, ub, wb);
     }
@@ -837,6 +861,8 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
     const bool all_active = (R + 1) * PB <= n;
     const int sw = ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
     const WarpBox box = warp_box(fa, pi, active);
+    // nucleons: every active target of the warp is a proton
+    const bool all_p = SIM == SIM_NUCLEON && box.has_p && __all_sync(0xffffffffu, !active || pi.w == 1.0);
     TargetAcc<PREC, MEAS> acc;
     acc.zero();
     // the mixed form on a box that allows it: FP32 displacements from the
@@ -891,15 +917,34 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
                     open_row(gm);
                     const float* tll = reinterpret_cast<const float*>(tl);
                     const double4* gsrc = bx.pos + (size_t)C * PB;
-                    if (full) {
-                        for (; gm; gm &= gm - 1)
-                            pair_group_nn_lo<MEAS, false>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
-                                                          diag, active, tid, sw, acc, my_acc);
-                    } else {
-                        for (; gm; gm &= gm - 1)
-                            pair_group_nn_lo<MEAS, true>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1), jlim,
-                                                         diag, active, tid, sw, acc, my_acc);
+                    // the species mode of this warp on this tile (pair_group_nn_lo)
+                    int mode = NN_ANY;
+                    if (!box.has_p && fa.nn_short) {
+                        mode = NN_NOP;
+                    } else if (all_p && gm) {
+                        bool any_n = false;
+#pragma unroll
+                        for (int blk = 0; blk < PB / 32; ++blk) {
+                            const int j = 32 * blk + lane;
+                            any_n |= j >= jmin && j < jlim && tlf[shadow_off(j, 3)] != 1.0f;
+                        }
+                        if (!__any_sync(0xffffffffu, any_n)) mode = NN_PP;
                     }
+                    auto run = [&](auto mode_c) {
+                        constexpr int MD = decltype(mode_c)::value;
+                        if (full) {
+                            for (; gm; gm &= gm - 1)
+                                pair_group_nn_lo<MEAS, false, MD>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1),
+                                                                  jlim, diag, active, tid, sw, acc, my_acc);
+                        } else {
+                            for (; gm; gm &= gm - 1)
+                                pair_group_nn_lo<MEAS, true, MD>(fa, si, nli, pi, tlf, tll, gsrc, 4 * (__ffs(gm) - 1),
+                                                                 jlim, diag, active, tid, sw, acc, my_acc);
+                        }
+                    };
+                    if (mode == NN_PP) run(std::integral_constant<int, NN_PP>());
+                    else if (mode == NN_NOP) run(std::integral_constant<int, NN_NOP>());
+                    else run(std::integral_constant<int, NN_ANY>());
                 }
                 if constexpr (PREC == PREC_MIXED && (SIM == SIM_PURE || SIM == SIM_MIX)) {
                     int kcode = -1;
