@@ -318,6 +318,8 @@ static void setup_args(yk_ctx* c)
             if ((double)tf > t) tf = std::nextafter(tf, 0.0f);
             f.hLm[k] = t > 0.0 ? tf : 0.0f;
         }
+        f.hLmin = std::min(f.hLm[0], std::min(f.hLm[1], f.hLm[2]));
+        f.coul_all = std::isinf(f.rc2f) ? 1 : 0;
     }
     f.n = c->n;
     f.nuclear_on = p.nuclear_on;

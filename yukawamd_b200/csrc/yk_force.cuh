@@ -81,6 +81,8 @@ struct ForceArgs {
     // minimum image instead (pair_group_nn_lo)
     int hilo;
     float hLm[3];
+    float hLmin;                     // the smallest hLm (a flag test against it flags a superset)
+    int coul_all;                    // the p-p Coulomb cutoff is beyond every FP32 distance (rc2f = inf)
 };
 
 // FP32 shadow positions ("posf") are stored tile by tile: tile t (slots
@@ -254,7 +256,7 @@ __device__ __forceinline__ float2 screen_d_x2(const ForceArgs& fa, const ScreenI
 }
 
 // screen_d_x2 for nucleons, also flagging (bits 0, 1 of flag for the two
-// pairs) the pairs whose hi-part displacement after the image shift is hLm
+// pairs) the pairs whose hi-part displacement after the image shift is hLmin
 // or more from 0 on some axis: the image decision of those pairs is close to
 // the reference's boundary |d| = L/2, and they take the exact FP64 image.
 __device__ __forceinline__ float2 screen_d_flag_x2(const ForceArgs& fa, const ScreenI& si, const float (&nli)[3],
@@ -264,7 +266,7 @@ __device__ __forceinline__ float2 screen_d_flag_x2(const ForceArgs& fa, const Sc
     const float2 MAG = make_float2(12582912.0f, 12582912.0f);
     const float2 NMAG = make_float2(-12582912.0f, -12582912.0f);
     const float ni[3] = {si.nx, si.ny, si.nz};
-    unsigned f = 0;
+    float2 mx = make_float2(0.f, 0.f);           // the largest |hi-part displacement| over the axes
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const float2 xj = *reinterpret_cast<const float2*>(t + c * 2 * SHADOW_TILE + 8 * g + off);
@@ -272,12 +274,14 @@ __device__ __forceinline__ float2 screen_d_flag_x2(const ForceArgs& fa, const Sc
         const float2 dc = __fadd2_rn(xj, make_float2(ni[c], ni[c]));
         const float2 k = __fadd2_rn(__ffma2_rn(dc, make_float2(fa.invLf[c], fa.invLf[c]), MAG), NMAG);
         const float2 d1 = __ffma2_rn(make_float2(-fa.Lh[c], -fa.Lh[c]), k, dc);       // exact
-        f |= (fabsf(d1.x) >= fa.hLm[c] ? 1u : 0u) | (fabsf(d1.y) >= fa.hLm[c] ? 2u : 0u);
+        mx = make_float2(fmaxf(mx.x, fabsf(d1.x)), fmaxf(mx.y, fabsf(d1.y)));
         float2 e = __fadd2_rn(lj, make_float2(nli[c], nli[c]));
         e = __ffma2_rn(make_float2(-fa.Ll[c], -fa.Ll[c]), k, e);
         d[c] = __fadd2_rn(d1, e);
     }
-    flag = f;
+    // against the smallest axis margin: in a box with unequal edges this also
+    // flags some pairs that do not need the exact image, which is only slower
+    flag = (mx.x >= fa.hLmin ? 1u : 0u) | (mx.y >= fa.hLmin ? 2u : 0u);
     float2 r2 = __fmul2_rn(d[2], d[2]);
     r2 = __ffma2_rn(d[1], d[1], r2);
     return __ffma2_rn(d[0], d[0], r2);
@@ -648,20 +652,24 @@ __device__ __forceinline__ void nuclear_terms_x2(const ForceArgs& fa, float2 r2,
     }
 }
 
-template <bool MEAS>
+// MASKED = false: every pair of the call takes the term (msk is ignored and
+// no pair may have r^2 = 0).
+template <bool MEAS, bool MASKED = true>
 __device__ __forceinline__ void coulomb_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2& fs, float2& u,
                                                  float2& w)
 {
-    const float2 r2s = make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f);
+    const float2 r2s = MASKED ? make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f) : r2;
     const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
     const float2 mr = __fmul2_rn(make_float2(fa.xmucf, fa.xmucf), __fmul2_rn(r2s, rinv));
     const float2 er = __fmul2_rn(__fmul2_rn(exp_neg_x2(mr), rinv), make_float2(fa.vcf, fa.vcf));
     // fc = (1 + mu r) q with q = er / r^2, masked
-    const float2 q = __fmul2_rn(er, __fmul2_rn(__fmul2_rn(rinv, rinv), msk));
+    const float2 rr = __fmul2_rn(rinv, rinv);
+    const float2 q = __fmul2_rn(er, MASKED ? __fmul2_rn(rr, msk) : rr);
     const float2 fc = __ffma2_rn(mr, q, q);
     fs = __fadd2_rn(fs, fc);
     if constexpr (MEAS) {
-        u = __ffma2_rn(__fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf)), msk, u);
+        const float2 ue = __fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf));
+        u = MASKED ? __ffma2_rn(ue, msk, u) : __fadd2_rn(u, ue);
         w = __ffma2_rn(fc, r2, w);
     }
 }

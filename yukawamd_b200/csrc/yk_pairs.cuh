@@ -402,8 +402,10 @@ __device__ __forceinline__ void pair_group_lo(const ForceArgs& fa, const ScreenI
 //   NN_NOP  no proton target (and fa.nn_short): no Coulomb term, and no flag
 //           test, since a pair near |d| = L/2 is beyond the nuclear range
 //           under either image;
-//   NN_PP   proton targets and proton sources only: every pair is a like pair
-//           and takes the Coulomb term, no species tests.
+//   NN_PP   proton targets and proton sources only, the Coulomb term on and
+//           uncut (fa.coul_all): every pair is a like pair and takes the
+//           Coulomb term, no species or cutoff tests (and on a full tile no
+//           masks in the Coulomb terms).
 constexpr int NN_ANY = 0, NN_NOP = 1, NN_PP = 2;
 
 template <bool MEAS, bool CHECK, int MODE = NN_ANY>
@@ -471,7 +473,11 @@ __device__ __forceinline__ void pair_group_nn_lo(const ForceArgs& fa, const Scre
     for (int jj = 0; jj < 4; ++jj) {
         const bool in = (ok >> jj) & 1u;
         if (in && fa.nuclear_on && r2v[jj] <= fa.rn2f) mn |= 1u << jj;
-        if (MODE != NN_NOP && in && fa.coulomb_on && ip && wj[jj] == 1.0f && r2v[jj] <= fa.rc2f) mc |= 1u << jj;
+        if constexpr (MODE == NN_PP) {
+            if (in) mc |= 1u << jj;
+        } else if constexpr (MODE == NN_ANY) {
+            if (in && fa.coulomb_on && ip && wj[jj] == 1.0f && r2v[jj] <= fa.rc2f) mc |= 1u << jj;
+        }
     }
     const bool any_n = __any_sync(0xffffffffu, mn != 0);
     const bool any_c = MODE != NN_NOP && __any_sync(0xffffffffu, mc != 0);
@@ -489,8 +495,12 @@ __device__ __forceinline__ void pair_group_nn_lo(const ForceArgs& fa, const Scre
         nuclear_terms_x2<MEAS>(fa, rb, make_float2((mn & 4u) ? 1.f : 0.f, (mn & 8u) ? 1.f : 0.f), Bb, fsb, ub, wb);
     }
     if (any_c) {
-        coulomb_terms_x2<MEAS>(fa, ra, make_float2((mc & 1u) ? 1.f : 0.f, (mc & 2u) ? 1.f : 0.f), fsa, ua, wa);
-        coulomb_terms_x2<MEAS>(fa, rb, make_float2((mc & 4u) ? 1.f : 0.f, (mc & 8u) ? 1.f : 0.f), fsb, ub, wb);
+        // proton pairs of a full tile: every pair takes the term, no masks
+        constexpr bool MASKED = !(MODE == NN_PP && !CHECK);
+        coulomb_terms_x2<MEAS, MASKED>(fa, ra, make_float2((mc & 1u) ? 1.f : 0.f, (mc & 2u) ? 1.f : 0.f), fsa, ua,
+                                       wa);
+        coulomb_terms_x2<MEAS, MASKED>(fa, rb, make_float2((mc & 4u) ? 1.f : 0.f, (mc & 8u) ? 1.f : 0.f), fsb, ub,
+                                       wb);
     }
     // F_i += fs (x_i - x_j) = -fs d (int_nn.f:230-240); the reaction on j is fs d
     GroupSum<PREC_MIXED, MEAS> gs;
@@ -921,7 +931,7 @@ __device__ __forceinline__ bool pairs_job(PairSmem<row_t<PREC>>& sm, const Force
                     int mode = NN_ANY;
                     if (!box.has_p && fa.nn_short) {
                         mode = NN_NOP;
-                    } else if (all_p && gm) {
+                    } else if (all_p && gm && fa.coul_all && fa.coulomb_on) {
                         bool any_n = false;
 #pragma unroll
                         for (int blk = 0; blk < PB / 32; ++blk) {
