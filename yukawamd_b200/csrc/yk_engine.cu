@@ -732,8 +732,12 @@ static int launch_force_t(yk_ctx* c)
                 c->pos, c->posf, pj, c->job_counter, c->fa, c->Si, Sj, c->Sm, c->err);
         }
     }
-    // dynamic shared memory: the unit flags of one row (M bytes at most)
-    const size_t fl_bytes = pj.Sjf ? (size_t)c->pj.M : 0;
+    // dynamic shared memory: the unit flags of one row and the list of its
+    // written rows (comb_smem_bytes); above 40 KB (M > 8,000 tiles, only on an
+    // explicit half-pair request past the scratch budget) it needs the opt-in
+    const size_t fl_bytes = pj.Sjf ? comb_smem_bytes(c->pj.M) : 0;
+    if (fl_bytes > (size_t)40 << 10)
+        cudaFuncSetAttribute(k_combine<SIM, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fl_bytes);
     k_combine<SIM, PREC><<<c->pj.M, COMB_THREADS, fl_bytes, c->stream>>>(c->Si, Sj, pj, c->perm, c->zii, c->aii,
                                                                          c->fa, c->a);
     return k;

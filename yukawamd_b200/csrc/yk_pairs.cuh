@@ -1177,6 +1177,13 @@ k_force_pairs(const double4* __restrict__ pos, const float* __restrict__ posf, P
 constexpr int COMB_GROUPS = 2;
 constexpr int COMB_THREADS = COMB_GROUPS * PB * 3;
 
+// Dynamic shared memory of k_combine for M tiles with unit flags: the flags of
+// the longest row (M bytes, padded to 4) and the list of its written rows.
+__host__ __device__ inline size_t comb_smem_bytes(int M)
+{
+    return (size_t)((M + 3) / 4) * 4 + sizeof(int) * (size_t)M;
+}
+
 template <int SIM, int PREC>
 __global__ void __launch_bounds__(COMB_THREADS)
 k_combine(const double* __restrict__ Si, const row_t<PREC>* __restrict__ Sj, PairJobs pj,
@@ -1184,7 +1191,10 @@ k_combine(const double* __restrict__ Si, const row_t<PREC>* __restrict__ Sj, Pai
           const double* __restrict__ aii, ForceArgs fa, double* __restrict__ a_out)
 {
     __shared__ double part[COMB_GROUPS][PB * 3];
-    extern __shared__ unsigned char sfl[];      // row R's unit flags (pj.Sjf), R + 1 bytes
+    __shared__ int nz_count;
+    // with pj.Sjf: row R's unit flags (R + 1 bytes, padded to 4) and then the
+    // list of its written rows in ascending order (comb_smem_bytes)
+    extern __shared__ int comb_dyn[];
     const int R = pj.M - 1 - (int)blockIdx.x;
     const int g = threadIdx.x / (PB * 3), t = threadIdx.x % (PB * 3);
     constexpr size_t ROW = (size_t)PB * 3;
@@ -1196,14 +1206,30 @@ k_combine(const double* __restrict__ Si, const row_t<PREC>* __restrict__ Sj, Pai
     const row_t<PREC>* sj = Sj + (size_t)tri_index(R, 0) * ROW + t;
     if (pj.Sjf) {
         // rows flagged zero were not written (k_force_pairs); skipping them
-        // leaves every sum as it was.  The flags are staged in shared memory
-        // first, so that the row loads of the unrolled loop issue together.
+        // leaves every sum as it was.  The flags are staged in shared memory,
+        // one warp lists the written rows in ascending order, and the groups
+        // take every COMB_GROUPS-th entry of the list: the row loads of the
+        // unrolled loop carry no condition and issue together.
+        unsigned char* sfl = reinterpret_cast<unsigned char*>(comb_dyn);
+        int* nzl = comb_dyn + (R + 4) / 4;
         const unsigned char* fl = pj.Sjf + tri_index(R, 0);
         for (int r = threadIdx.x; r <= R; r += blockDim.x) sfl[r] = fl[r];
         __syncthreads();
-#pragma unroll 4
-        for (int R2 = g; R2 <= R; R2 += COMB_GROUPS)
-            if (sfl[R2]) F += (double)sj[(size_t)R2 * ROW];
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            int cnt = 0;
+            for (int b = 0; b <= R; b += 32) {
+                const bool on = b + lane <= R && sfl[b + lane] != 0;
+                const unsigned m = __ballot_sync(0xffffffffu, on);
+                if (on) nzl[cnt + __popc(m & ((1u << lane) - 1u))] = b + lane;
+                cnt += __popc(m);
+            }
+            if (lane == 0) nz_count = cnt;
+        }
+        __syncthreads();
+        const int cnt = nz_count;
+#pragma unroll 8
+        for (int q = g; q < cnt; q += COMB_GROUPS) F += (double)sj[(size_t)nzl[q] * ROW];
     } else {
 #pragma unroll 4
         for (int R2 = g; R2 <= R; R2 += COMB_GROUPS) F += (double)sj[(size_t)R2 * ROW];
