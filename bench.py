@@ -244,6 +244,71 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class NvmlClockSampler:
+    """SM clock and clock-event reasons of one GPU read through NVML every
+    `period_s` from a host thread, started and stopped around the timed steps
+    only, so that every sample falls inside the timed region (nvidia-smi's
+    shortest period is longer than a whole 20-step run).  Read-only queries."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, uuid, period_s=0.002):
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = None
+        # torch reports the UUID without NVML's "GPU-" prefix: match by substring
+        for k in range(pynvml.nvmlDeviceGetCount()):
+            hk = pynvml.nvmlDeviceGetHandleByIndex(k)
+            u = pynvml.nvmlDeviceGetUUID(hk)
+            u = u.decode() if isinstance(u, bytes) else u
+            if uuid and uuid in u:
+                self.h = hk
+                break
+        if self.h is None:
+            raise RuntimeError("no NVML device with UUID %s" % uuid)
+        self.period = period_s
+        self.samples = []
+        self.bits = 0
+        self._stop = threading.Event()
+        self.thread = None
+
+    def _poll(self):
+        nv = self.nv
+        read_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                self.bits |= int(read_reasons(self.h))
+            except nv.NVMLError:
+                pass
+            time.sleep(self.period)
+
+    def start(self):
+        self._stop.clear()
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        self._stop.set()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def result(self):
+        nv = self.nv
+        if not self.samples:
+            return None
+        smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        reasons = sorted(name for name, const in self.REASONS if self.bits & int(getattr(nv, const, 0)))
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": float(smax), "reasons": reasons,
+                "samples": len(self.samples), "sampler": "NVML every %.0f ms during the timed steps"
+                                                         % (1e3 * self.period)}
+
+
 def device_uuid(dev):
     try:
         import torch
@@ -258,7 +323,7 @@ def device_uuid(dev):
 KERNEL_CHOICE = [0]       # --kernel: 0 auto, 1 rows, 2 pairs, 3 near lists
 
 
-def time_engine(w, precision, steps, warmup, meas_every, dist, flush=True):
+def time_engine(w, precision, steps, warmup, meas_every, dist, flush=True, sampler=None):
     """W untimed steps, then K timed steps; returns (ms_total, perf, launches)."""
     from yukawamd_b200 import abi
     from yukawamd_b200.engine import Engine, kernel_launch_count
@@ -276,7 +341,11 @@ def time_engine(w, precision, steps, warmup, meas_every, dist, flush=True):
     e.perf_enable(True, L2_FLUSH_BYTES if flush else 0)
     dist.barrier()
     l0 = kernel_launch_count()
+    if sampler is not None:
+        sampler.start()
     e.run(steps, meas_every, series=False)
+    if sampler is not None:
+        sampler.stop()
     launches = kernel_launch_count() - l0
     dist.barrier()
     perf = e.perf_read()
@@ -429,10 +498,15 @@ def run_ours(args, dist):
     K, W, me = args.steps, args.warmup, args.meas_every
 
     uuid = device_uuid(dist.local)
-    clocks = ClockSampler(uuid)
-    clocks.start()
-    e, perf, launches = time_engine(w, args.precision, K, W, me, dist)
-    clk = clocks.stop()
+    try:
+        nvs = NvmlClockSampler(uuid)
+    except Exception:
+        nvs = None
+    if nvs is None:
+        clocks = ClockSampler(uuid)
+        clocks.start()
+    e, perf, launches = time_engine(w, args.precision, K, W, me, dist, sampler=nvs)
+    clk = nvs.result() if nvs is not None else clocks.stop()
     ms_local = perf.run_ms
     ms = dist.max(ms_local)
     value = job_rate(dist.world, pairs_step * K, ms)
