@@ -130,36 +130,27 @@ __global__ void k_b_repack(const int* __restrict__ iperm, const int* __restrict_
     store_pos(pos, posf, iperm[o], xn, zii[o]);
 }
 
-// vel_verlet_2.f:33-54 for every box (block table: box, block within box;
-// entries of box -1 are unused), in the caller's order: every read and
-// write is coalesced.  The slot-ordered copies follow in k_b_pack.
+// vel_verlet_2.f:33-54 for every box, one thread per element (component
+// e % 3 of the box's particle e / 3), in the caller's order: three CTAs per
+// entry of the block table (box, block within box; entries of box -1 are
+// unused), each over a contiguous third of the block's 3 VBLOCK elements, so
+// every warp access is 256 contiguous bytes and the three loads of a thread
+// are independent.  The slot-ordered copies follow in k_b_pack.
 __global__ void __launch_bounds__(VBLOCK)
 k_b_drift(const int2* __restrict__ vb, const RepDesc* __restrict__ rd, const int* __restrict__ left,
           double* __restrict__ x, double* __restrict__ v, double* __restrict__ vold, const double* __restrict__ a)
 {
-    const int2 t = vb[blockIdx.x];
+    const int2 t = vb[blockIdx.x / 3];
     if (t.x < 0 || left[t.x] <= 0) return;
     const RepDesc* d = rd + t.x;
-    const int local = t.y * VBLOCK + threadIdx.x;
-    const StepArgs s = d->sa;
-    if (local >= s.n) return;
-    const int gi = d->P + local;
-    const double* ar = a + d->A;
-    // all nine loads before the first store (they are then in flight together)
-    double xi[3], vi[3], ai[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        xi[k] = x[3 * gi + k];
-        vi[k] = v[3 * gi + k];
-        ai[k] = ar[3 * local + k];
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int e = 3 * gi + k;
-        x[e] = drift1(xi[k], vi[k], ai[k], s, k);
-        vold[e] = vi[k];
-        v[e] = __dadd_rn(vi[k], __dmul_rn(s.dt, ai[k]));
-    }
+    const int le = 3 * VBLOCK * t.y + (int)(blockIdx.x % 3) * VBLOCK + threadIdx.x;   // element in the box
+    const StepArgs& s = d->sa;
+    if (le >= 3 * s.n) return;
+    const size_t e = 3 * (size_t)d->P + le;
+    const double xi = x[e], vi = v[e], ai = a[d->A + le];
+    x[e] = drift1(xi, vi, ai, s, le % 3);
+    vold[e] = vi;
+    v[e] = __dadd_rn(vi, __dmul_rn(s.dt, ai));
 }
 
 // The slot-ordered FP64 positions and FP32 shadow of every box that steps, a
@@ -540,7 +531,7 @@ static int enqueue_step_b(yk_batch* b, bool meas, bool series, bool resort)
         b->pos_dirty = false;
         ++k;
     }
-    k_b_drift<<<b->vb_cap, VBLOCK, 0, st>>>(b->vblocks, b->rd, b->left, b->x, b->v, b->vold, b->a);
+    k_b_drift<<<3 * b->vb_cap, VBLOCK, 0, st>>>(b->vblocks, b->rd, b->left, b->x, b->v, b->vold, b->a);
     k_b_pack<<<(b->tcap * PB + 255) / 256, 256, 0, st>>>(b->tile_rep, b->rd, b->left, b->perm, b->x, b->zii,
                                                           b->pos, b->posf, b->tcap * PB);
     k += 2;
