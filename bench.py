@@ -71,6 +71,9 @@ def parse():
                          "precision and report the total-energy drift")
     ap.add_argument("--kernel", choices=["auto", "rows", "pairs", "near"], default="auto",
                     help="force kernel (default: the engine's automatic choice)")
+    ap.add_argument("--equilibrate", type=int, default=3,
+                    help="groups of 100 untimed FP64 steps (cancel_vcom + tnorm after each, md.F:87-101) "
+                         "that bring every timed box to its run state before the warm-up steps")
     ap.add_argument("--drift-warmup", type=int, default=20,
                     help="warm-up groups of 100 steps (cancel_vcom + tnorm after each) before --drift")
     ap.add_argument("--ensemble-steps", type=int, default=100)
@@ -104,6 +107,24 @@ def make_workload(kind, seed, n=0):
     if kind == "ocp":
         return configs.pure_ion_ocp(seed, **kw)
     return configs.nucleon_matter(seed, **kw)
+
+
+def equilibrate(w, groups, dist):
+    """The workload with its positions and velocities after md.F's warm-up
+    (`groups` groups of 100 FP64 steps, each followed by cancel_vcom and
+    tnorm, md.F:87-101): the state a long run spends its steps in.  The
+    uniform random start has pairs closer than the liquid allows, and timing
+    its first steps would time a box that is not yet the run's."""
+    if groups <= 0:
+        return w
+    import dataclasses
+    from yukawamd_b200 import abi
+    from yukawamd_b200.driver import RunControl, run_md
+    from yukawamd_b200.engine import Engine
+    with Engine(w, device=dist.local, precision=abi.YK_PREC_FP64) as e:
+        run_md(e, RunControl(nwgroup=groups, nwsteps=100))
+        x, v, _vold, _a = e.get_state()
+    return dataclasses.replace(w, x=np.ascontiguousarray(x), v=np.ascontiguousarray(v))
 
 
 def workload_desc(w, kind):
@@ -493,7 +514,8 @@ def run_ours(args, dist):
     from yukawamd_b200 import _lib
     from yukawamd_b200.engine import peak_probe
     kind = args.workload
-    w = make_workload(kind, args.seed + dist.rank, args.n)
+    w0 = make_workload(kind, args.seed + dist.rank, args.n)
+    w = equilibrate(w0, args.equilibrate, dist)
     pairs_step = w.pairs_per_step
     K, W, me = args.steps, args.warmup, args.meas_every
 
@@ -535,7 +557,8 @@ def run_ours(args, dist):
            "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if args.precision == "fp64" else "f64+f32",
            "data": "synthetic: numpy PCG64 seed %d (+rank), uniform positions, Maxwell "
-                   "velocities with zero momentum" % args.seed,
+                   "velocities with zero momentum, then %d untimed groups of 100 FP64 steps with "
+                   "cancel_vcom + tnorm (md.F warm-up)" % (args.seed, args.equilibrate),
            "config": {"workload": workload_desc(w, kind), "n": w.n,
                       "pairs_per_step": pairs_step, "precision": args.precision,
                       "integrator": "vel_verlet_2", "meas_every": me,
@@ -584,10 +607,10 @@ def run_ours(args, dist):
             out["mixed"]["vs_oracle"] = mixed_vs_oracle(w)
 
     if not args.no_extras and dist.world == 1:
-        out["nucleon"] = nucleon_pair(K, W, me, dist)
+        out["nucleon"] = nucleon_pair(K, W, me, dist, args.equilibrate)
         out["ensemble"] = ensemble(args.ensemble_steps, me, dist)
         if args.line_drift_steps > 0:
-            out["drift"] = drift_block(w, kind, args.line_drift_steps, args.drift_warmup, dist)
+            out["drift"] = drift_block(w0, kind, args.line_drift_steps, args.drift_warmup, dist)
         if not args.no_served:
             out["served"] = served_ensemble(args, dist)
 
@@ -682,12 +705,13 @@ def served_ensemble(args, dist):
     return rep
 
 
-def nucleon_pair(K, W, me, dist):
+def nucleon_pair(K, W, me, dist, groups=0):
     """int_nn.f at N = 51,200 (proton fraction 0.4, n_B = 0.05 fm^-3, kT = 1
-    MeV): FP64 and mixed pairs/s and the mixed form's accuracy."""
+    MeV): FP64 and mixed pairs/s and the mixed form's accuracy, from the state
+    after `groups` md.F warm-up groups."""
     from yukawamd_b200 import abi
     from yukawamd_b200.engine import Engine
-    w = make_workload("nucleon", 3 + dist.rank)
+    w = equilibrate(make_workload("nucleon", 3 + dist.rank), groups, dist)
     res = {"workload": workload_desc(w, "nucleon"), "pairs_per_step": w.pairs_per_step}
     for prec in ("fp64", "mixed"):
         e, perf, _ = time_engine(w, prec, K, W, me, dist)
@@ -785,11 +809,13 @@ def serve_ensemble(args, dist):
 
 def tune_report(args, dist):
     """The autotuner (yukawamd_b200/tune.py) on the benchmark workloads: for
-    each single box every candidate's force-call time (CUDA events) and the
-    winner; for the replica ensemble every job segment length's graph time."""
+    each single box every candidate's step and force-call times (CUDA events,
+    16 steps) and the winner (shortest step); for the replica ensemble every
+    job segment length's graph time."""
     from yukawamd_b200 import abi, configs, tune
     from yukawamd_b200.engine import Batch, Engine
-    out = {"metric": "autotuner: force-call ms per candidate (single boxes), graph ms per 50 steps (ensemble)"}
+    out = {"metric": "autotuner: step ms and force-call ms per candidate (single boxes), graph ms per 50 steps "
+                     "(ensemble)"}
     for name, w in (("ocp_4096", configs.pure_ion_ocp(1)), ("mix_55296", configs.ion_mixture_cfg(2)),
                     ("nucleon_51200", configs.nucleon_matter(3))):
         for prec in ("fp64", "mixed"):
@@ -798,8 +824,9 @@ def tune_report(args, dist):
                 e.accel(True)
                 best, best_ms, res = tune.tune(e, device=dist.local, save=False)
             out["%s_%s" % (name, prec)] = {
-                "winner": best, "force_ms": best_ms,
-                "tried": [[r[0] if r[0] != float("inf") else None, r[1]] for r in res]}
+                "winner": best, "step_ms": best_ms,
+                "tried": [[r[0] if r[0] != float("inf") else None, r[1],
+                           r[3] if r[3] != float("inf") else None] for r in res]}
     boxes = configs.replica_ensemble(4)
     with Batch(boxes, device=dist.local, precision=abi.YK_PREC_MIXED) as b:
         b.accel(True)

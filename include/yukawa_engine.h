@@ -306,7 +306,8 @@ typedef struct yk_tuning {
     int pair_seg;         /* longest job of the half-pair kernels, in source
                              tiles (jobs shrink towards the end of the job
                              list); 0 = automatic (8 FP64, 4 mixed)         */
-    int sort_every;       /* steps between Hilbert re-orderings (-1 = never)  */
+    int sort_every;       /* steps between Hilbert re-orderings (-1 = never,
+                             0 = automatic: 4)                              */
     int graph_steps;      /* steps captured per CUDA graph by yk_run          */
     int source_split;     /* CTAs of the half-pair kernel (2, or auto when it
                              picks 2) that share one 128-target block, each
@@ -327,10 +328,10 @@ YK_API int yk_get_tuning(yk_ctx* ctx, yk_tuning* out);
 YK_API int yk_set_tuning(yk_ctx* ctx, const yk_tuning* t);
 
 /* The batch's tunables: pair_seg (source tiles per job, all boxes) and
- * graph_steps (steps per CUDA graph of yk_batch_run; the batch re-sorts at
- * the start of every graph, which yk_batch_get_tuning reports as
- * sort_every).  force_kernel must be 0 or 2.  Changing pair_seg rebuilds
- * the job table and its scratch. */
+ * graph_steps (steps per CUDA graph of yk_batch_run) and sort_every (steps
+ * between the boxes' Hilbert re-orderings, counted from the start of each
+ * graph, which always re-sorts; 0 = automatic: 4).  force_kernel must be 0
+ * or 2.  Changing pair_seg rebuilds the job table and its scratch. */
 YK_API int yk_batch_get_tuning(yk_batch* b, yk_tuning* out);
 YK_API int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t);
 

@@ -160,25 +160,30 @@ def test_f64_exp_within_three_ulp():
     assert exp_neg_f64(701.0) == 0.0
 
 
-def test_rsqrt_newton_two_steps_error_bound():
-    """rsqrt_nr64 (yukawamd_b200/csrc/yk_common.cuh): two FP64 Newton steps
-    y <- y (3/2 - (x/2) y^2) from an FP32 estimate.  Restated in numpy with
-    the estimate off by up to 2^-21 relative either way (the hardware's is
-    within about 2^-22), over r^2 from 1e-4 to 1e9: the result is within 4 ulp
-    of 1/sqrt(x) (computed to 50 digits)."""
+def test_rsqrt_second_order_error_bound():
+    """rsqrt_nr64 (yukawamd_b200/csrc/yk_common.cuh): one second-order
+    correction y + y e (1/2 + 3e/8), e = fma(-(x y), y, 1), of an FP32
+    estimate y.  Restated with each FMA rounded once (exact rational
+    arithmetic, then one rounding to double) and the estimate off by up to
+    2^-21 relative either way (the hardware's is within about 2^-22), over
+    r^2 from 1e-4 to 1e9: the result is within 1 ulp of 1/sqrt(x) (computed
+    to 50 digits)."""
     from decimal import Decimal, getcontext
+    from fractions import Fraction
     getcontext().prec = 50
+
+    def fma(a, b, c):
+        return float(Fraction(a) * Fraction(b) + Fraction(c))
+
     rng = np.random.default_rng(11)
     xs = np.concatenate([10.0 ** rng.uniform(-4, 9, 400), [1.0, 2.0, 0.25, 8.9e4, 1e9]])
     worst = 0.0
     for x in xs:
-        exact = float(1 / Decimal(float(x)).sqrt())
+        x = float(x)
+        exact = float(1 / Decimal(x).sqrt())
         for rel in (-2.0 ** -21, 0.0, 2.0 ** -21, rng.uniform(-2.0 ** -21, 2.0 ** -21)):
-            y = np.float64(np.float32(exact * (1.0 + rel)))
-            h = np.float64(0.5) * np.float64(x)
-            for _ in range(2):
-                hy = h * y
-                e = np.float64(1.5) - hy * y          # one FMA on the device: at most as far off
-                y = y * e
-            worst = max(worst, abs(y - exact) / np.spacing(exact))
-    assert worst <= 4.0, worst
+            y = float(np.float32(exact * (1.0 + rel)))
+            e = fma(-(x * y), y, 1.0)
+            r = fma(y * e, fma(e, 0.375, 0.5), y)
+            worst = max(worst, abs(r - exact) / np.spacing(exact))
+    assert worst <= 1.0, worst

@@ -57,6 +57,11 @@ namespace {
 
 constexpr int BATCH_SEG = 8;
 constexpr int BATCH_GRAPH_STEPS = 50;
+// Steps between the boxes' re-orderings inside a graph (each graph starts
+// with one): the single-box engine's cadence, for the same reason (the warp
+// boxes grow as particles move away from their sorted neighbours).
+constexpr int BATCH_SORT_EVERY = 4;
+constexpr int SORT_AT_GRAPH_START_ONLY = INT_MAX;
 constexpr int BATCH_MAX_GRAPHS = 8;
 constexpr int UNLIMITED = INT_MAX;   // step budget of the boxes of yk_batch_create
 
@@ -421,6 +426,8 @@ struct yk_batch {
     int force_grid = 0, force_grid_lo = 0;
     bool all_lo = false;            // every held box allows the mixed hi/lo displacement (fa.lo / fa.hilo)
     int seg = BATCH_SEG, graph_steps = BATCH_GRAPH_STEPS;
+    int sort_every = BATCH_SORT_EVERY;
+    int since_sort = 0;             // steps run since the last re-ordering (eager steps)
     std::vector<RepDesc> hrd;       // host copy of the descriptors
     bool pos_dirty = false;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -596,7 +603,8 @@ static GraphB* graph_b(yk_batch* b, int K, int me, int phase, bool series, int* 
         return nullptr;
     }
     int kernels = 0;
-    for (int l = 1; l <= K; ++l) kernels += enqueue_step_b(b, me > 0 && (phase + l) % me == 0, series, l == 1);
+    for (int l = 1; l <= K; ++l)
+        kernels += enqueue_step_b(b, me > 0 && (phase + l) % me == 0, series, (l - 1) % b->sort_every == 0);
     e = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) {
         *rc = bfail(b, YK_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
@@ -930,7 +938,7 @@ int yk_batch_get_tuning(yk_batch* b, yk_tuning* out)
     if (!b || !out) return bfail(b, YK_ERR_ARG, "batch and out are required");
     out->force_kernel = 2;
     out->pair_seg = b->seg;
-    out->sort_every = b->graph_steps;       // the batch re-sorts at the start of every graph
+    out->sort_every = b->sort_every == SORT_AT_GRAPH_START_ONLY ? -1 : b->sort_every;
     out->graph_steps = b->graph_steps;
     out->source_split = 1;
     out->targets_per_thread = 1;
@@ -942,7 +950,7 @@ int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t)
     if (!b || !t) return bfail(b, YK_ERR_ARG, "batch and tuning are required");
     if (t->force_kernel != 0 && t->force_kernel != 2)
         return bfail(b, YK_ERR_UNSUPPORTED, "a batch runs the half-pair kernel (force_kernel 0 or 2)");
-    if (t->pair_seg < 0 || t->graph_steps < 0) return bfail(b, YK_ERR_ARG, "bad tuning values");
+    if (t->pair_seg < 0 || t->graph_steps < 0 || t->sort_every < -1) return bfail(b, YK_ERR_ARG, "bad tuning values");
     if (t->source_split > 1) return bfail(b, YK_ERR_UNSUPPORTED, "a batch runs whole source tiles (source_split 0 or 1)");
     if (t->targets_per_thread > 1)
         return bfail(b, YK_ERR_UNSUPPORTED, "a batch runs one target per thread (targets_per_thread 0 or 1)");
@@ -950,6 +958,8 @@ int yk_batch_set_tuning(yk_batch* b, const yk_tuning* t)
     BCK(b, cudaStreamSynchronize(b->stream));
     drop_graphs_b(b);
     b->graph_steps = t->graph_steps > 0 ? t->graph_steps : BATCH_GRAPH_STEPS;
+    // -1: only at the start of each graph
+    b->sort_every = t->sort_every > 0 ? t->sort_every : t->sort_every < 0 ? SORT_AT_GRAPH_START_ONLY : BATCH_SORT_EVERY;
     const int seg = t->pair_seg > 0 ? t->pair_seg : BATCH_SEG;
     if (seg == b->seg) return YK_OK;
     if (seg < b->cap_seg) {
@@ -1244,7 +1254,10 @@ int yk_batch_accel(yk_batch* b, int do_meas, yk_scalars* out)
     BCK(b, cudaSetDevice(b->dev));
     const bool meas = do_meas != 0;
     int k = 0;
-    if (b->pos_dirty) k += enqueue_sort(b, false);
+    if (b->pos_dirty) {
+        k += enqueue_sort(b, false);
+        b->since_sort = 0;
+    }
     k += enqueue_force_b(b, meas);
     k_b_finish<<<b->nslots, 256, 0, b->stream>>>(b->rd, nullptr, b->left, b->Sm, b->kpart, b->a, b->ds, nullptr,
                                                  b->series_idx, b->nslots, meas ? 1 : 0, 0, 0);
@@ -1285,7 +1298,10 @@ int yk_batch_run(yk_batch* b, int nsteps, int meas_every, yk_scalars* series, do
     const int me = meas_every;
     const int K = b->graph_steps;
     int k = 0, s = 1;
-    if (b->pos_dirty) k += enqueue_sort(b, false);
+    if (b->pos_dirty) {
+        k += enqueue_sort(b, false);
+        b->since_sort = 0;
+    }
     while (s + K - 1 <= nsteps) {
         int rc = YK_OK;
         GraphB* g = graph_b(b, K, me, me > 0 ? (s - 1) % me : 0, want, &rc);
@@ -1293,8 +1309,14 @@ int yk_batch_run(yk_batch* b, int nsteps, int meas_every, yk_scalars* series, do
         BCK(b, cudaGraphLaunch(g->exec, st));
         k += g->kernels;
         s += K;
+        // the graph's last re-ordering was at its step 1 + se floor((K - 1) / se)
+        b->since_sort = (K - 1) % b->sort_every + 1;
     }
-    for (; s <= nsteps; ++s) k += enqueue_step_b(b, me > 0 && s % me == 0, want, false);
+    for (; s <= nsteps; ++s) {
+        const bool resort = b->since_sort >= b->sort_every;
+        k += enqueue_step_b(b, me > 0 && s % me == 0, want, resort);
+        b->since_sort = resort ? 1 : b->since_sort + 1;
+    }
     BCK(b, cudaEventRecord(b->e1, st));
     count_launches(k);
     int rc = sync_check_b(b);

@@ -349,17 +349,17 @@ __device__ __forceinline__ double exp_neg_f64(double t)
 }
 
 // FP64 1/sqrt(x) for x > 0 inside the FP32 normal range (a pair's r^2, or 1
-// for a masked pair): Newton's iteration y <- y (3/2 - (x/2) y^2) from the FP32
-// hardware estimate.  Each step squares the relative error (about 2^-22 ->
-// 2^-43 -> below the FP64 rounding), so two steps leave the rounding errors
-// of the steps themselves, a few ulp.
+// for a masked pair): one second-order correction of the FP32 hardware
+// estimate y.  With e = 1 - x y^2 (one FMA, exact but for the rounding of
+// x y), 1/sqrt(x) = y (1 - e)^(-1/2) = y (1 + e/2 + 3e^2/8 + 5e^3/16 + ...);
+// |e| is about 2^-21, so the dropped terms are below 2^-63 relative and the
+// result is within about 1 ulp: five FP64 instructions at a dependency depth
+// of four, against seven at depth six for two Newton steps.
 __device__ __forceinline__ double rsqrt_nr64(double x)
 {
-    double y = (double)rsqrtf(__double2float_rn(x));
-    const double h = 0.5 * x;
-    y = __dmul_rn(y, __fma_rn(-__dmul_rn(h, y), y, 1.5));
-    y = __dmul_rn(y, __fma_rn(-__dmul_rn(h, y), y, 1.5));
-    return y;
+    const double y = (double)rsqrtf(__double2float_rn(x));
+    const double e = __fma_rn(-__dmul_rn(x, y), y, 1.0);
+    return __fma_rn(__dmul_rn(y, e), __fma_rn(e, 0.375, 0.5), y);
 }
 
 // FP32 1/sqrt(x): hardware estimate plus one Newton step.

@@ -16,7 +16,7 @@
 //         species equality; Coulomb (p-p, r^2 <= rccut^2): vc x the ion terms.
 //
 // PREC_FP64: all FP64 (exp_neg_f64, our table-driven exp; for ions
-// rsqrt_nr64, Newton's iteration from the FP32 hardware estimate, for the
+// rsqrt_nr64, a second-order correction of the FP32 hardware estimate, for the
 // nucleon Coulomb term the library rsqrt; the reciprocal root replaces the
 // reference's sqrt and divide, 1/(r r^2) = rinv^3).
 // PREC_MIXED: the r^2, rsqrt, exp and force terms in FP32.  Pairs take their
@@ -367,8 +367,9 @@ __device__ __forceinline__ void phys64(const ForceArgs& fa, double wi, double wj
         }
         if (fa.coulomb_on && wi == 1.0 && wj == 1.0 && r2 <= fa.rc2) {
             // the library root: on this branchy single-pair path the longer
-            // dependency chain of rsqrt_nr64 made the 51,200-nucleon step
-            // 3.5 % slower (the ion paths interleave four pairs and gain 2 %)
+            // dependency chain of two Newton steps from the FP32 estimate
+            // made the 51,200-nucleon step 3.5 % slower (the ion paths
+            // interleave four pairs and gained 2 %)
             const double rinv = rsqrt(r2);
             const double r = r2 * rinv;
             const double mr = fa.xmuc * r;

@@ -252,12 +252,14 @@ class Batch:
         check_batch(self._lib.yk_batch_get_tuning(self._b, C.byref(t)), self._b)
         return t
 
-    def set_tuning(self, pair_seg=None, graph_steps=None):
+    def set_tuning(self, pair_seg=None, graph_steps=None, sort_every=None):
         t = self.tuning()
         if pair_seg is not None:
             t.pair_seg = int(pair_seg)
         if graph_steps is not None:
             t.graph_steps = int(graph_steps)
+        if sort_every is not None:
+            t.sort_every = int(sort_every)
         check_batch(self._lib.yk_batch_set_tuning(self._b, C.byref(t)), self._b)
         return self.tuning()
 

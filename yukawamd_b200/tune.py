@@ -8,10 +8,12 @@ kernel that evaluates each pair from both sides), cap the half-pair jobs at
 target, for small boxes), give each thread one or two targets
 (`targets_per_thread`: target blocks of 128 or 256 slots, the tile shape of
 the ion kernels); it refreshes
-the Morton order every `sort_every` steps.  Which choice is fastest depends on
+the Hilbert order every `sort_every` steps.  Which choice is fastest depends on
 N, the cutoff radius relative to the box, the interaction and the precision,
 so the tuner measures candidates on the caller's own workload (CUDA-event
-time of the force call, yk_perf) and remembers the winner per
+time per step, sorts included, yk_perf, over a window of 16 steps: the force
+call slows down step by step after a sort as particles leave their
+neighbours, which a shorter window would not see) and remembers the winner per
 
     (GPU name, sim type, precision, N bucket)      N bucket = round(2 log2 N)
 
@@ -25,25 +27,29 @@ import time
 
 from . import abi
 
+# sort_every 0 is the engine's automatic cadence (4 steps)
 CANDIDATES = [
-    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=8, sort_every=50),
-    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=4, sort_every=50),
-    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=16, sort_every=50),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=50),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=4, sort_every=50),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=16, sort_every=50),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=2, sort_every=50),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=20),
+    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=8, sort_every=0),
+    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=4, sort_every=0),
+    dict(force_kernel=abi.KERNEL_NEAR, pair_seg=16, sort_every=0),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=0),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=4, sort_every=0),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=16, sort_every=0),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=2, sort_every=0),
+    # re-sort cadence
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=8),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=16),
     dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=-1),
-    dict(force_kernel=abi.KERNEL_ROWS, pair_seg=8, sort_every=50),
+    dict(force_kernel=abi.KERNEL_ROWS, pair_seg=8, sort_every=0),
     # threads per target: 2 or 4 CTAs share each 128-target block (small boxes)
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=50, source_split=2),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=50, source_split=4),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=0, source_split=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=1, sort_every=0, source_split=4),
     # tile shape: two targets per thread (256-target blocks; ion boxes on the
     # FP64 exact-image or mixed hi/lo path, others fall back to one)
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=50, targets_per_thread=2),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=4, sort_every=50, targets_per_thread=2),
-    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=16, sort_every=50, targets_per_thread=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=8, sort_every=0, targets_per_thread=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=4, sort_every=0, targets_per_thread=2),
+    dict(force_kernel=abi.KERNEL_PAIRS, pair_seg=16, sort_every=0, targets_per_thread=2),
 ]
 # source_split > 1 makes one job per unit and part: only worth trying while the
 # box has few tiles (it is there to fill the GPU with a small box)
@@ -92,22 +98,25 @@ def key_for(engine, device=0):
     return "%s|sim%d|prec%d|nb%d" % (gpu_name(device), p.sim_type, p.precision, bucket(engine.n))
 
 
-def measure(engine, cand, steps=6, warmup=2):
-    """Mean CUDA-event time (ms) of the force call under candidate `cand`.
-    The engine's state advances by warmup + steps steps."""
+def measure(engine, cand, steps=16, warmup=2):
+    """Mean CUDA-event times (ms) per step (sorts included) and per force call
+    under candidate `cand`.  The engine's state advances by warmup + steps
+    steps."""
     engine.set_tuning(**cand)
     engine.run(warmup, 0, series=False)
     engine.perf_enable(True, 0)
     engine.run(steps, 0, series=False)
     perf = engine.perf_read()
     engine.perf_enable(False, 0)
-    return perf.force_ms / max(perf.force_calls, 1)
+    return perf.run_ms / max(perf.steps, 1), perf.force_ms / max(perf.force_calls, 1)
 
 
-def tune(engine, candidates=None, steps=6, warmup=2, device=0, save=True):
+def tune(engine, candidates=None, steps=16, warmup=2, device=0, save=True):
     """Time every candidate on this engine's workload; apply and return the
-    best one.  The engine's positions are restored afterwards, so tuning does
-    not advance the caller's trajectory."""
+    one with the shortest step (the result's ms) and the list of (step ms,
+    candidate, error or None, force-call ms).  The engine's positions are
+    restored afterwards, so tuning does not advance the caller's
+    trajectory."""
     candidates = candidates or [c for c in CANDIDATES
                                 if c.get("source_split", 1) == 1 or engine.n <= SPLIT_MAX_N]
     x, v, vold, a = engine.get_state()
@@ -117,18 +126,18 @@ def tune(engine, candidates=None, steps=6, warmup=2, device=0, save=True):
         cand.setdefault("source_split", 1)
         cand.setdefault("targets_per_thread", 1)
         try:
-            ms = measure(engine, cand, steps, warmup)
+            ms, fms = measure(engine, cand, steps, warmup)
         except Exception as exc:          # e.g. scratch too large for this N
-            results.append((float("inf"), cand, str(exc)))
+            results.append((float("inf"), cand, str(exc), float("inf")))
             continue
-        results.append((ms, cand, None))
+        results.append((ms, cand, None, fms))
         engine.set_state(x=x, v=v, vold=vold, a=a)
-    best_ms, best, _ = min(results, key=lambda r: r[0])
+    best_ms, best, _, best_fms = min(results, key=lambda r: r[0])
     engine.set_tuning(**best)
     engine.set_state(x=x, v=v, vold=vold, a=a)
     if save:
         doc = _load()
-        doc[key_for(engine, device)] = dict(best, force_ms=best_ms, when=time.time(),
+        doc[key_for(engine, device)] = dict(best, step_ms=best_ms, force_ms=best_fms, when=time.time(),
                                             n=engine.n, tried=[(r[0], r[1]) for r in results])
         _store(doc)
     return best, best_ms, results
