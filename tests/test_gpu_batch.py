@@ -127,6 +127,29 @@ def test_batch_rejects_mixed_kinds(gpu):
     assert ei.value.code == abi.YK_ERR_ARG
 
 
+def test_sort_cadence_changes_nothing_but_speed(gpu):
+    """sort_every only sets when the slot order is refreshed.  The engine's
+    default is 4; a batch's tuning round-trips (0 -> the automatic 4, -1 ->
+    only at the start of each graph); and 23 steps in graphs of 10 plus 3
+    eager steps (where the batch counts the steps since its last sort) end
+    at the same positions under every cadence, to summation-order
+    rounding."""
+    boxes = ion_boxes()
+    with Engine(boxes[1]) as e:
+        assert e.tuning().sort_every == 4
+    res = {}
+    for se in (0, 1, 7, -1):
+        with Batch(boxes, mix_mode=abi.YK_MIX_FIXED) as b:
+            t = b.set_tuning(graph_steps=10, sort_every=se)
+            assert t.sort_every == {0: 4, -1: -1}.get(se, se) and t.graph_steps == 10
+            b.accel(True)
+            b.run(23, 5, series=False)
+            res[se] = [b.get_state(r)[0] for r in range(b.nrep)]
+    for se in (1, 7, -1):
+        for r in range(len(boxes)):
+            assert _rel(res[se][r], res[0][r]) <= 1e-12, (se, r)
+
+
 def test_batch_tuning_changes_nothing_but_speed(gpu):
     """pair_seg only re-cuts the work items: accelerations agree with the
     default cut to summation-order rounding, and a graph run after the
