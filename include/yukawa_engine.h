@@ -308,7 +308,10 @@ typedef struct yk_tuning {
                              list); 0 = automatic (8 FP64, 4 mixed)         */
     int sort_every;       /* steps between Hilbert re-orderings (-1 = never,
                              0 = automatic: 4)                              */
-    int graph_steps;      /* steps captured per CUDA graph by yk_run          */
+    int graph_steps;      /* steps per CUDA graph of yk_run: the graphs take
+                             the most whole multiples of u that fit (at least
+                             one), u = sort_every or, when it is at most
+                             4 graph_steps, lcm(sort_every, meas_every)    */
     int source_split;     /* CTAs of the half-pair kernel (2, or auto when it
                              picks 2) that share one 128-target block, each
                              taking a contiguous 1/split of every source tile,

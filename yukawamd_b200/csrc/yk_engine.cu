@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <numeric>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -1420,11 +1421,17 @@ int yk_run(yk_ctx* c, int nsteps, int meas_every, yk_scalars* series)
         return finish_run(c, nsteps, want_series, series);
     }
     // Eager steps until the step count is aligned with the sort cadence,
-    // then graphs of K steps (K a multiple of sort_every), then the rest.
+    // then graphs of K steps, then the rest.  K is a multiple of sort_every
+    // and, when that keeps the graph within 4 graph_steps, of meas_every
+    // too, so that every graph of the run starts at the same measuring
+    // phase and one captured graph serves them all.
     int s = 1;
-    const int K = c->sort_every > 0
-                      ? c->sort_every * std::max(1, c->graph_steps / c->sort_every)
-                      : c->graph_steps;
+    int unit = c->sort_every > 0 ? c->sort_every : 1;
+    if (me > 0) {
+        const long long l = (long long)unit / std::gcd(unit, me) * me;
+        if (l <= 4LL * std::max(c->graph_steps, unit)) unit = (int)l;
+    }
+    const int K = c->sort_every > 0 || me > 0 ? unit * std::max(1, c->graph_steps / unit) : c->graph_steps;
     while (s <= nsteps && c->sort_every > 0 && c->step_count % c->sort_every != 0) {
         k += enqueue_newton(c, meas_at(s), want_series, sort_due(c, c->step_count));
         c->step_count += 1;
