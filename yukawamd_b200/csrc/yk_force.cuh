@@ -600,17 +600,22 @@ __device__ __forceinline__ void ion_pair_f32(const ForceArgs& fa, float r2, bool
 // the instruction's own error (about 2 ulp) for the pairs that carry the
 // force (mu r of a few), and about 6e-7 at the cutoff mu r = 10, where the
 // term is weighted by e^-10; fs = q (1 + mu r) with q = e^{-mu r} / r^3.
+// A masked pair takes r^2 = 1e36 instead of a multiply by the mask: then
+// q = e^{-mu r} 1e-54 rounds to exactly 0 in FP32 for any mu >= 0 (1/r and
+// 1/r^2 stay normal numbers, mu r finite), so fs = 0 (one FP32x2 multiply
+// fewer per two pairs: mixed step 1.000 -> 0.983 ms).
 template <bool MEAS>
 __device__ __forceinline__ void ion_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2& fs, float2& u,
                                              float2& w)
 {
     const float L2E = 1.44269502162933349609375f;           // float(log2 e)
-    const float2 r2s = make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f);
+    const float FAR = 1e36f;
+    const float2 r2s = make_float2(msk.x != 0.f ? r2.x : FAR, msk.y != 0.f ? r2.y : FAR);
     const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
     const float2 mr = __fmul2_rn(make_float2(fa.xmucf, fa.xmucf), __fmul2_rn(r2s, rinv));
     const float2 y = __fmul2_rn(mr, make_float2(-L2E, -L2E));
     const float2 er = __fmul2_rn(make_float2(ex2_approx(y.x), ex2_approx(y.y)), rinv);
-    const float2 q = __fmul2_rn(er, __fmul2_rn(__fmul2_rn(rinv, rinv), msk));
+    const float2 q = __fmul2_rn(er, __fmul2_rn(rinv, rinv));
     fs = __ffma2_rn(mr, q, q);
     if constexpr (MEAS) {
         u = __fmul2_rn(__fadd2_rn(er, make_float2(-fa.evcutf, -fa.evcutf)), msk);
