@@ -664,13 +664,15 @@ template <bool MEAS, bool MASKED = true>
 __device__ __forceinline__ void coulomb_terms_x2(const ForceArgs& fa, float2 r2, float2 msk, float2& fs, float2& u,
                                                  float2& w)
 {
-    const float2 r2s = MASKED ? make_float2(msk.x != 0.f ? r2.x : 1.0f, msk.y != 0.f ? r2.y : 1.0f) : r2;
+    // a masked pair takes r^2 = 1e36 (as in ion_terms_x2): q rounds to 0
+    const float FAR = 1e36f;
+    const float2 r2s = MASKED ? make_float2(msk.x != 0.f ? r2.x : FAR, msk.y != 0.f ? r2.y : FAR) : r2;
     const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
     const float2 mr = __fmul2_rn(make_float2(fa.xmucf, fa.xmucf), __fmul2_rn(r2s, rinv));
     const float2 er = __fmul2_rn(__fmul2_rn(exp_neg_x2(mr), rinv), make_float2(fa.vcf, fa.vcf));
-    // fc = (1 + mu r) q with q = er / r^2, masked
+    // fc = (1 + mu r) q with q = er / r^2
     const float2 rr = __fmul2_rn(rinv, rinv);
-    const float2 q = __fmul2_rn(er, MASKED ? __fmul2_rn(rr, msk) : rr);
+    const float2 q = __fmul2_rn(er, rr);
     const float2 fc = __ffma2_rn(mr, q, q);
     fs = __fadd2_rn(fs, fc);
     if constexpr (MEAS) {
