@@ -187,3 +187,27 @@ def test_rsqrt_second_order_error_bound():
             r = fma(y * e, fma(e, 0.375, 0.5), y)
             worst = max(worst, abs(r - exact) / np.spacing(exact))
     assert worst <= 1.0, worst
+
+
+def test_far_mask_rounds_the_pair_term_to_zero():
+    """ion_terms_x2 and coulomb_terms_x2 (yukawamd_b200/csrc/yk_force.cuh)
+    give a masked pair r^2 = 1e36 instead of multiplying its term by the
+    mask.  Restated in numpy float32 with the reciprocal-root estimate off by
+    up to 2^-21 either way: 1/r and 1/r^2 stay normal, mu r stays finite, and
+    q = prefactor e^{-mu r} (1/r)^3 is exactly 0 for every mu >= 0 (mu = 0,
+    unscreened, included) and prefactors up to 1e6, so fs = mu r q + q = 0."""
+    f32 = np.float32
+    r2s = f32(1e36)
+    for rel in (-2.0 ** -21, 0.0, 2.0 ** -21):
+        rinv = f32(f32(1.0 / np.sqrt(1e36)) * f32(1.0 + rel))
+        rr = f32(rinv * rinv)
+        assert rr >= np.finfo(np.float32).tiny
+        for mu in (0.0, 1e-3, 0.1, 10.0):
+            mr = f32(f32(mu) * f32(r2s * rinv))
+            assert np.isfinite(mr)
+            e = f32(np.exp2(np.float64(mr) * -1.4426950408889634))   # 0 unless mu = 0
+            for pre in (1.0, 1.44, 1e6):
+                er = f32(f32(e * rinv) * f32(pre))
+                q = f32(er * rr)
+                assert q == 0.0, (rel, mu, pre, q)
+                assert f32(mr * q + q) == 0.0
